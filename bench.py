@@ -1,0 +1,361 @@
+"""Throughput of the SIMP loop on B200: SIMP iterations/s and DOF*CG-iterations/s.
+
+Workload (default, one GPU): the 128x64x64 cantilever with a protected-void
+cylinder (radius 12, axis y, centre x=64, z=32), a protected-solid slab
+x in [0, 4), volfrac 0.3, penal 3, rmin 3, beta 1, eta 0.5, move 0.2,
+unit-cube elements, total unit -z load on the x=nelx, z=0 edge.  A "step" is
+one iteration of the loop body: multigrid-PCG solve, sensitivities, OC
+bisection, re-projection.  Synthetic inputs, no dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+Under torchrun every rank runs an independent replica (the path has no data
+exchange); ``value`` is the whole-job rate (sum over ranks at the max-over-ranks
+time).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NELX, NELY, NELZ = 128, 64, 64
+VOLFRAC, PENAL, RMIN, BETA, ETA, MOVE = 0.3, 3.0, 3.0, 1.0, 0.5, 0.2
+
+
+def workload(nelx=NELX, nely=NELY, nelz=NELZ):
+    """Masks and loads of the 128x64x64 configuration (scaled for other sizes)."""
+    from pytopo3d_b200.assembly import build_force_vector, build_supports
+
+    shape = (nely, nelx, nelz)
+    yy, xx, zz = np.ogrid[:nely, :nelx, :nelz]
+    r = 12 * nelx // 128
+    void = np.broadcast_to((xx - nelx // 2) ** 2 + (zz - nelz // 2) ** 2 <= r * r, shape).copy()
+    solid = np.zeros(shape, bool)
+    solid[:, : max(1, 4 * nelx // 128), :] = True
+    solid[:, -1, 0] = True  # load strip (optimizer.py:366-369)
+    solid[:, 0, :] = True  # support face (optimizer.py:378-390)
+    solid &= ~void
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    F = build_force_vector(nelx, nely, nelz, ndof) / (nely + 1)  # total unit load
+    free, _ = build_supports(nelx, nely, nelz, ndof)
+    fixed = np.ones(ndof, np.uint8)
+    fixed[free] = 0
+    return shape, solid, void, F, fixed
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_loop(precision, x0=None):
+    from pytopo3d_b200.optimizer import SimpLoop
+    from pytopo3d_b200.stiffness import lk_H8
+
+    shape, solid, void, F, fixed = workload()
+    loop = SimpLoop(NELX, NELY, NELZ, VOLFRAC, PENAL, RMIN, lk_H8(elem_size=1.0), F, fixed, solid, void,
+                    projection_eta=ETA, move=MOVE, precision=precision, x0=x0)
+    loop.set_beta(BETA)
+    return loop
+
+
+def time_device_steps(loop, steps, dist):
+    import torch
+
+    L = __import__("pytopo3d_b200._lib", fromlist=["lib"]).lib()
+    cg = 0
+    barrier(dist)
+    torch.cuda.synchronize()
+    n0 = L.tp3d_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    cs = []
+    for _ in range(steps):
+        st = loop.step()
+        cg += loop.last["cg_iterations"]
+        cs.append(st[:1])
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms = e0.elapsed_time(e1)
+    launches = L.tp3d_launch_count() - n0
+    c = float(cs[-1].item())
+    return ms, cg, launches, c
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(v, dist):
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_sample(steps=1):
+    """The reference algorithm (oracle restatement: COO/CSR assembly, SuperLU spsolve,
+    element energy, chain rule, OC bisection) timed on the host cores.  The
+    128x64x64 direct solve does not fit (SuperLU fill on 1.6 M DOF), so the
+    sample is the same loop body at 32x16x16, where the reference runs."""
+    from oracle import simp_oracle as O
+
+    nelx, nely, nelz = 32, 16, 16
+    shape = (nely, nelx, nelz)
+    solid, void, free = O.prepare_masks(nelx, nely, nelz)
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    F = O.build_force_vector(nelx, nely, nelz, ndof) / (nely + 1)
+    freedofs, _ = O.build_supports(nelx, nely, nelz, ndof)
+    KE = O.lk_H8(elem_size=1.0)
+    H, Hs = O.build_filter(nelx, nely, nelz, RMIN)
+    x = np.full(shape, VOLFRAC)
+    x[solid], x[void] = 1.0, 0.0
+    target = VOLFRAC * int(free.sum())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _, rho, dp = O.build_physical_density(x, H, Hs, BETA, ETA, solid, void)
+        it = O.simp_iteration(x, rho, dp, BETA, ETA, PENAL, MOVE, target, H, Hs, KE, F, freedofs, solid, void,
+                              free, nelx, nely, nelz)
+        x = it["x_new"]
+    dt = time.perf_counter() - t0
+    return steps / dt, dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    steps = max(1, args.steps)
+    warm = min(1, args.warmup)
+    if warm:
+        cpu_reference_sample(1)
+    rate, dt = cpu_reference_sample(steps)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    line = {
+        "impl": "reference", "metric": "SIMP iterations/s", "value": rate, "unit": "iter/s", "n_gpus": 0,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "cantilever 32x16x16 (reference CPU path: SuperLU spsolve); the 128x64x64 "
+                               "workload does not fit the reference's direct solve", "beta": BETA,
+                   "rmin": RMIN, "volfrac": VOLFRAC},
+        "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": 1, "kind": "port",
+                         "sample": f"{steps} loop bodies of the oracle restatement at 32x16x16 "
+                                   f"(single-threaded SuperLU), {cores} cores visible"},
+        "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    from pytopo3d_b200 import _lib
+
+    L = _lib.lib()
+    W = max(3, args.warmup)
+    results = {}
+    for prec in ([args.precision] + [p for p in ("fp64", "mixed") if p != args.precision]):
+        loop = make_loop(prec)
+        for _ in range(W):
+            loop.step()
+        torch.cuda.synchronize()
+        if prec == args.precision:
+            with ClockSampler(local) as clk:
+                ms, cg, launches, c = time_device_steps(loop, args.steps, dist)
+            clocks = clk.summary()
+        else:
+            ms, cg, launches, c = time_device_steps(loop, max(3, args.steps // 4), dist)
+        steps = args.steps if prec == args.precision else max(3, args.steps // 4)
+        ms = max_over_ranks(ms, dist)
+        apply_ms = (ctypes_time_apply(loop.solver, fp32=(prec == "mixed")))
+        results[prec] = dict(ms=ms, steps=steps, cg=cg, launches=launches, c=c, apply_ms=apply_ms,
+                             loop=loop, stats=loop.solver.stats())
+        if prec != args.precision:
+            loop.close()
+
+    main_r = results[args.precision]
+    loop = main_r["loop"]
+    ndof = 3 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
+    nele = NELX * NELY * NELZ
+    steps = main_r["steps"]
+    rate = world * steps / (main_r["ms"] / 1e3)
+
+    # end-to-end through the public API with host buffers (pinned H2D of x, D2H of x_new + c)
+    x_host = loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
+    for _ in range(2):
+        x_host, _ = loop.step_host(x_host)
+    barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_steps = max(3, args.steps // 2)
+    for _ in range(e_steps):
+        x_host, c_host = loop.step_host(x_host)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_rate = world * e_steps / e2e_s
+
+    # roofline of the dominant kernel (fine-level operator apply)
+    peak, peak_kind = peaks()
+    fp32 = args.precision == "mixed"
+    alg_bytes = (8 * ndof + 2 * nele) if fp32 else (16 * ndof + 8 * nele)
+    achieved = alg_bytes / (main_r["apply_ms"] * 1e-3) / 1e9
+    flops = 1152.0 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("fine_apply_" + ("f32" if fp32 else "f64"))
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        crate, cdt = cpu_reference_sample(1)
+        cpu = {"value": crate, "unit": "iter/s", "cores": 1, "kind": "port",
+               "sample": "1 loop body of the oracle restatement at 32x16x16 (SuperLU spsolve, single "
+                         "thread); the 128x64x64 direct solve does not fit the reference's CPU path"}
+
+    other = [p for p in results if p != args.precision]
+    line = {
+        "metric": "SIMP iterations/s", "value": rate, "unit": "iter/s", "n_gpus": world, "steps": steps,
+        "warmup": W, "ms_per_step": main_r["ms"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+bf16 inner / f64 refinement" if fp32 else "f64",
+        "data": "synthetic",
+        "config": {"workload": "cantilever 128x64x64, void cylinder r12 (axis y), solid slab x<4, beta 1",
+                   "nele": nele, "ndof": ndof, "precision": args.precision, "rmin": RMIN,
+                   "volfrac": VOLFRAC, "l2": "working set (multigrid hierarchy + vectors) > 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "dof_cg_iters_per_s": world * ndof * main_r["cg"] / (main_r["ms"] / 1e3),
+        "cg_iterations_per_step": main_r["cg"] / steps,
+        "compliance": main_r["c"],
+        "solver": {k: v for k, v in main_r["stats"].items()},
+        "other_precision": {p: {"value": world * results[p]["steps"] / (results[p]["ms"] / 1e3),
+                                "cg_iterations_per_step": results[p]["cg"] / results[p]["steps"],
+                                "apply_ms": results[p]["apply_ms"]} for p in other},
+        "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": 8 * nele,
+                "d2h_bytes_per_step": 8 * nele + 8},
+        "roofline": {"bound": "hbm", "kernel": "fine_apply_kernel<" + ("float" if fp32 else "double") + ">",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic, "bytes_per_launch": alg_bytes,
+                     "launch_ms": main_r["apply_ms"],
+                     "flop_rate_tflops": flops / (main_r["apply_ms"] * 1e-3) / 1e12},
+        "cpu_baseline": cpu,
+        "gpu_launches": main_r["launches"],
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    loop.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_time_apply(solver, fp32):
+    import ctypes
+
+    from pytopo3d_b200 import _lib
+
+    ms = ctypes.c_double(0)
+    _lib.check(_lib.lib().tp3d_solver_time_apply(solver._h, 1 if fp32 else 0, 20, ctypes.byref(ms)),
+               "time_apply")
+    return ms.value
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,174 @@
+/*
+ * topo3d_b200 — C ABI of the B200 (sm_100a) SIMP hot path.
+ *
+ * Every entry point takes plain device pointers and sizes plus a `void*`
+ * CUDA stream (NULL = legacy default stream) and returns an int status:
+ *   0  ok,  >0 not converged / iteration cap,  <0 bad argument or CUDA error.
+ * `tp3d_last_error()` returns a thread-local message for the last failure.
+ *
+ * Array conventions (all follow PyTopo3D):
+ *   element arrays: length nelx*nely*nelz, Fortran order of the (nely, nelx,
+ *     nelz) design array, e = y + nely*(x + nelx*z)   (pytopo3d/utils/filter.py:85-87)
+ *   node / DOF vectors: DOF = 3*(iy + (nely+1)*(ix + (nelx+1)*iz)) + c
+ *     (pytopo3d/utils/assembly.py:121-129, 375-401)
+ *   masks: uint8, nonzero = true.
+ * The caller owns every buffer passed in.  Solver handles own their scratch
+ * and multigrid hierarchy; a handle belongs to one stream and one thread.
+ */
+#ifndef TOPO3D_B200_H
+#define TOPO3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TP3D_OK 0
+#define TP3D_NOT_CONVERGED 1
+#define TP3D_ERR_ARG (-1)
+#define TP3D_ERR_CUDA (-2)
+#define TP3D_ERR_TIMEOUT (-3)   /* a bounded device-side wait expired */
+#define TP3D_ERR_NONFINITE (-4) /* NaN / Inf met in a reduction */
+
+#define TP3D_PRECISION_FP64 0  /* FP64 everywhere */
+#define TP3D_PRECISION_MIXED 1 /* FP32 inner PCG + BF16 density, FP64 refinement */
+
+const char* tp3d_last_error(void);
+int tp3d_abi_version(void);
+
+/* Kernel launches issued by this library since load (CUDA-graph replays add
+ * their kernel-node count).  Instrumentation; no reference counterpart. */
+long long tp3d_launch_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Density filter and Heaviside projection
+ * ------------------------------------------------------------------------- */
+
+/* Row sums Hs of the cone filter, zero sums replaced by 1.
+ * Replaces build_filter's Hs (pytopo3d/utils/filter.py:122-228); the matrix H
+ * itself is never formed: every filter entry point applies the same cone
+ * weights rmin - |d| > 1e-9 as a stencil. */
+int tp3d_filter_rowsum(int nelx, int nely, int nelz, double rmin, double* Hs, void* stream);
+
+/* rho_filtered = (H x) / Hs, projected and clamped on protected regions.
+ * Replaces build_physical_density (pytopo3d/utils/filter.py:63-100) and
+ * heaviside_projection (filter.py:26-60).  rho_filtered and dproj may be NULL;
+ * solid / void_ may be NULL (no protected elements). */
+int tp3d_filter_project(int nelx, int nely, int nelz, double rmin, const double* x,
+                        const double* Hs, double beta, double eta, const uint8_t* solid,
+                        const uint8_t* void_, double* rho_filtered, double* rho_physical,
+                        double* dproj, void* stream);
+
+/* out = H^T (g * dproj / Hs).  Replaces apply_density_filter_chain_rule
+ * (pytopo3d/utils/filter.py:103-119).  dproj may be NULL (treated as 1). */
+int tp3d_filter_transpose(int nelx, int nely, int nelz, double rmin, const double* g,
+                          const double* dproj, const double* Hs, double* out, void* stream);
+
+/* Elementwise tanh projection and its derivative, n values.
+ * Replaces heaviside_projection (pytopo3d/utils/filter.py:26-60). */
+int tp3d_heaviside(const double* rho_filtered, long long n, double beta, double eta, double* out,
+                   double* derivative, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Element energy and sensitivities
+ * ------------------------------------------------------------------------- */
+
+/* ce[e] = u_e^T KE u_e.  KE is 24x24 row-major on the HOST.
+ * Replaces element_compliance (pytopo3d/core/compliance.py:18-75). */
+int tp3d_element_compliance(int nelx, int nely, int nelz, const double* U, const double* KE_host,
+                            double* ce, void* stream);
+
+/* Fused loop-body sensitivities (pytopo3d/core/optimizer.py:596-625):
+ *   ce, compliance = sum (Emin + (1-Emin) rho^p) ce  (written to *compliance, device),
+ *   dc_dx = H^T(dc dproj / Hs) with dc = -p (1-Emin) rho^(p-1) ce,
+ *   dv_dx = H^T(free dproj / Hs).
+ * ce may be NULL.  `scratch` holds >= tp3d_sensitivity_scratch_bytes() bytes of
+ * device memory. */
+size_t tp3d_sensitivity_scratch_bytes(int nelx, int nely, int nelz);
+int tp3d_sensitivity(int nelx, int nely, int nelz, double rmin, const double* U,
+                     const double* KE_host, const double* rho_physical, const double* dproj,
+                     const double* Hs, const uint8_t* free_mask, double penal, double* ce,
+                     double* dc_dx, double* dv_dx, double* compliance, void* scratch,
+                     void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Optimality-criteria update with projected-volume bisection
+ * ------------------------------------------------------------------------- */
+
+/* Replaces optimality_criteria_update_projected (pytopo3d/utils/oc_update.py:25-124).
+ * The whole lambda bisection runs in one cooperative launch; each step
+ * re-filters and re-projects the candidate on the device.
+ * stats (device, 8 doubles): [lambda_best, volume_best, steps, change,
+ *   ratio_scale, lambda_lo, lambda_hi, best_error].
+ * change = max |x_new - x| over free elements (optimizer.py:642).
+ * `scratch` holds >= tp3d_oc_scratch_bytes() bytes of device memory. */
+size_t tp3d_oc_scratch_bytes(int nelx, int nely, int nelz, double rmin);
+int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const double* x,
+                   const double* dc_dx, const double* dv_dx, const double* Hs,
+                   const uint8_t* solid, const uint8_t* void_, double move,
+                   double target_free_volume, double beta, double eta, int max_bisection,
+                   double bisection_tol, double* x_new, double* rho_new, double* stats,
+                   void* scratch, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Matrix-free H8 elasticity solver (multigrid-preconditioned CG)
+ * ------------------------------------------------------------------------- */
+
+typedef struct tp3d_solver tp3d_solver;
+
+typedef struct tp3d_solver_opts {
+  int precision;        /* TP3D_PRECISION_FP64 or TP3D_PRECISION_MIXED */
+  int max_iterations;   /* PCG iterations (FP64) / inner iterations per refinement step */
+  double rtol;          /* target ||f - K u|| / ||f|| */
+  int pre_sweeps;       /* smoother sweeps before restriction */
+  int post_sweeps;      /* smoother sweeps after prolongation */
+  double omega;         /* damped-Jacobi weight (<=0: Chebyshev) */
+  int coarsest_max_dofs;/* stop coarsening at or below this many DOFs */
+  int max_levels;       /* cap on multigrid levels (1 = Jacobi-PCG only) */
+  double inner_rtol;    /* mixed: inner FP32 PCG tolerance per refinement step */
+  int max_refinements;  /* mixed: cap on FP64 refinement steps */
+} tp3d_solver_opts;
+
+void tp3d_solver_default_opts(tp3d_solver_opts* opts);
+
+/* Create a solver for a (nelx, nely, nelz) grid.  KE_host: 24x24 row-major
+ * host array (lk_H8, pytopo3d/utils/stiffness.py:12-130).  fixed_dofs: device
+ * uint8 per DOF (the complement of build_supports' freedofs,
+ * pytopo3d/utils/assembly.py:224-348). */
+int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host,
+                       const uint8_t* fixed_dofs, const tp3d_solver_opts* opts, void* stream,
+                       tp3d_solver** out);
+int tp3d_solver_destroy(tp3d_solver* s);
+
+/* Set the SIMP moduli E = Emin + (1-Emin) rho^penal (optimizer.py:584-586) and
+ * rebuild the multigrid hierarchy.  rho_physical: device, nele doubles. */
+int tp3d_solver_set_density(tp3d_solver* s, const double* rho_physical, double penal);
+
+/* Solve K(rho) U = F on the free DOFs; fixed DOFs of U are set to 0.
+ * U holds the initial guess on entry.  Replaces the assembly + solver_func
+ * call (optimizer.py:584-594, pytopo3d/utils/solver.py:43-73).
+ * iterations / relres: host out-params (may be NULL). */
+int tp3d_solver_solve(tp3d_solver* s, const double* F, double* U, int* iterations,
+                      double* relres);
+
+/* y = K u with fixed rows/cols replaced by identity (FP64 / FP32 forms). */
+int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
+int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
+
+/* Average device time (ms) of the fine-level operator kernel over `launches`
+ * back-to-back launches on the solver's stream, timed with CUDA events around
+ * them (fp32 != 0: the mixed-precision FP32/BF16 kernel).  Measurement helper
+ * for the roofline figure; no reference counterpart. */
+int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch);
+
+/* Diagnostics of the last solve: [levels, iterations, refinements, relres,
+ * inner_iterations_total, coarsest_dofs, ...]; returns the count written. */
+int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOPO3D_B200_H */

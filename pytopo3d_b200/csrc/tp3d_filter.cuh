@@ -1,0 +1,138 @@
+// Cone density filter as a shared-memory stencil.
+//
+// The reference builds an explicit sparse H with weights rmin - |d| for
+// integer offsets d with rmin - |d| > 1e-9, truncated at the domain boundary
+// (pytopo3d/utils/filter.py:122-228).  H is symmetric, so H x and H^T g are the
+// same stencil.  Here H is never formed: a block stages a (32 + 2Z) x (TX + 2Z)
+// x (KZ + 2Z) tile of the input (zero outside the domain, which reproduces the
+// boundary truncation) in shared memory, and each thread produces KZ outputs
+// along z.  Taps are grouped in (dx, dy) columns so each staged value is loaded
+// once per column and reused for all KZ outputs.
+#pragma once
+
+#include "tp3d_common.cuh"
+
+namespace tp3d {
+
+constexpr int kFilterTY = 32;   // outputs along y per block (one warp)
+constexpr int kFilterTX = 8;    // outputs along x per block (warps per block)
+constexpr int kFilterKZ = 8;    // outputs along z per thread
+constexpr int kFilterThreads = kFilterTY * kFilterTX;
+constexpr int kFilterMaxZ = 6;  // supports rmin <= 7
+
+struct FilterCols {
+  const int2* dxy;    // (dx, dy) per column
+  const double* w;    // ncols x (2Z+1) weights, 0 where the tap is absent
+  int ncols;
+  int Z;              // max |offset| along any axis
+};
+
+// Host: columns for a radius, cached per (device, rmin).  Returns nonzero on error.
+int filter_cols_for(double rmin, FilterCols* out);
+
+__host__ __device__ inline int filter_smem_elems(int Z) {
+  return (kFilterTY + 2 * Z) * (kFilterTX + 2 * Z) * (kFilterKZ + 2 * Z);
+}
+
+struct FilterTile {
+  int x0, y0, z0;
+};
+
+__host__ __device__ inline int filter_tiles_x(const Grid& g) { return (g.nx + kFilterTX - 1) / kFilterTX; }
+__host__ __device__ inline int filter_tiles_y(const Grid& g) { return (g.ny + kFilterTY - 1) / kFilterTY; }
+__host__ __device__ inline int filter_tiles_z(const Grid& g) { return (g.nz + kFilterKZ - 1) / kFilterKZ; }
+__host__ __device__ inline long long filter_ntiles(const Grid& g) {
+  return (long long)filter_tiles_x(g) * filter_tiles_y(g) * filter_tiles_z(g);
+}
+__device__ inline FilterTile filter_tile_at(const Grid& g, long long t) {
+  const int ty = filter_tiles_y(g), tx = filter_tiles_x(g);
+  FilterTile r;
+  r.y0 = (int)(t % ty) * kFilterTY;
+  t /= ty;
+  r.x0 = (int)(t % tx) * kFilterTX;
+  r.z0 = (int)(t / tx) * kFilterKZ;
+  return r;
+}
+
+// Stage `load(e, x, y, z)` (called only for in-domain elements) into `s`.
+template <int Z, class Load>
+__device__ __forceinline__ void filter_stage(const Grid& g, const FilterTile& t, double* s, Load load) {
+  constexpr int SY = kFilterTY + 2 * Z, SX = kFilterTX + 2 * Z, SZ = kFilterKZ + 2 * Z;
+  for (int i = threadIdx.x; i < SY * SX * SZ; i += blockDim.x) {
+    const int ly = i % SY;
+    const int r = i / SY;
+    const int lx = r % SX, lz = r / SX;
+    const int gx = t.x0 + lx - Z, gy = t.y0 + ly - Z, gz = t.z0 + lz - Z;
+    double v = 0.0;
+    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz)
+      v = load(g.eidx(gx, gy, gz), gx, gy, gz);
+    s[i] = v;
+  }
+}
+
+// Apply the staged stencil; calls `store(e, x, y, z, value)` for in-domain outputs.
+template <int Z, class Store>
+__device__ __forceinline__ void filter_apply(const Grid& g, const FilterCols& fc, const FilterTile& t,
+                                             const double* s, Store store) {
+  constexpr int SY = kFilterTY + 2 * Z, SX = kFilterTX + 2 * Z;
+  constexpr int W = 2 * Z + 1;
+  const int ly = threadIdx.x % kFilterTY, lx = threadIdx.x / kFilterTY;
+  double acc[kFilterKZ];
+#pragma unroll
+  for (int k = 0; k < kFilterKZ; ++k) acc[k] = 0.0;
+  for (int c = 0; c < fc.ncols; ++c) {
+    const int2 d = __ldg(&fc.dxy[c]);
+    const double* wc = fc.w + (size_t)c * W;
+    double wv[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j) wv[j] = __ldg(&wc[j]);
+    const double* col = s + (size_t)(lx + Z + d.x) * SY + (ly + Z + d.y);
+    double v[kFilterKZ + 2 * Z];
+#pragma unroll
+    for (int j = 0; j < kFilterKZ + 2 * Z; ++j) v[j] = col[(size_t)j * SX * SY];
+#pragma unroll
+    for (int k = 0; k < kFilterKZ; ++k) {
+#pragma unroll
+      for (int j = 0; j < W; ++j) acc[k] = fma(wv[j], v[k + j], acc[k]);
+    }
+  }
+  const int gx = t.x0 + lx, gy = t.y0 + ly;
+  if (gx < g.nx && gy < g.ny) {
+#pragma unroll
+    for (int k = 0; k < kFilterKZ; ++k) {
+      const int gz = t.z0 + k;
+      if (gz < g.nz) store(g.eidx(gx, gy, gz), gx, gy, gz, acc[k]);
+    }
+  }
+}
+
+// Heaviside projection (pytopo3d/utils/filter.py:26-60).
+struct Projection {
+  double beta, eta, tbe, den;
+  __host__ Projection(double b, double e) : beta(b), eta(e) {
+    tbe = tanh(b * e);
+    den = tanh(b * e) + tanh(b * (1.0 - e));
+  }
+  // Same operation order as the reference: divide by the denominator.
+  __device__ __forceinline__ double value(double rf, double* deriv) const {
+    const double t = tanh(beta * (rf - eta));
+    if (deriv) *deriv = beta * (1.0 - t * t) / den;
+    const double r = (tbe + t) / den;
+    return fmin(fmax(r, 0.0), 1.0);
+  }
+};
+
+// Dispatch a templated launcher on Z at runtime.
+#define TP3D_DISPATCH_Z(Zval, ...)                      \
+  switch (Zval) {                                       \
+    case 0: { constexpr int ZC = 0; __VA_ARGS__; } break; \
+    case 1: { constexpr int ZC = 1; __VA_ARGS__; } break; \
+    case 2: { constexpr int ZC = 2; __VA_ARGS__; } break; \
+    case 3: { constexpr int ZC = 3; __VA_ARGS__; } break; \
+    case 4: { constexpr int ZC = 4; __VA_ARGS__; } break; \
+    case 5: { constexpr int ZC = 5; __VA_ARGS__; } break; \
+    case 6: { constexpr int ZC = 6; __VA_ARGS__; } break; \
+    default: return TP3D_ERR_ARG;                       \
+  }
+
+}  // namespace tp3d

@@ -1,0 +1,409 @@
+// Matrix-free trilinear-hexahedron elasticity operator and multigrid kernels.
+//
+// Replaces the reference's per-iteration CSR assembly (kron + add.at + the
+// K[free][:,free] slice, pytopo3d/core/optimizer.py:584-591) and the sparse
+// direct / CG solve (pytopo3d/utils/solver.py:15-73).
+//
+// Fine level: y = Z K(E) Z u + (I - Z) u, applied node by node from the 24x24
+// element stiffness KE (kernel-parameter space, i.e. the constant bank, so
+// every FMA takes its coefficient as an immediate-bank operand) and the
+// element moduli E.  Z masks fixed DOFs.  A block owns a TY x TX column of
+// nodes and marches along z; each step stages one new node plane of u (tile +
+// 1 halo) and one element slab of E in shared memory.  Per node the 27
+// neighbours are read once and fed into 8 per-element accumulators (576 FMAs
+// per node, 24 independent FMA chains).
+//
+// Coarse levels: Galerkin operators P^T A P of the unmasked stiffness with
+// trilinear P, stored as 27-point 3x3-block stencils (243 coefficients per
+// node, structure-of-arrays), fixed DOFs by injection.
+#pragma once
+
+#include "tp3d_common.cuh"
+
+namespace tp3d {
+
+template <typename T>
+struct KEP {
+  T k[576];
+};
+
+// ----------------------------------------------------------------------------
+// per-element modulus sources
+// ----------------------------------------------------------------------------
+struct EFromF64 {
+  const double* E;
+  __device__ __forceinline__ double operator()(long long e) const { return __ldg(&E[e]); }
+};
+struct EFromBF16 {
+  const __nv_bfloat16* rho;
+  float penal;
+  __device__ __forceinline__ float operator()(long long e) const {
+    const float r = __bfloat162float(rho[e]);
+    const float rp = (penal == 3.0f) ? r * r * r : powf(r, penal);
+    return 1.0e-9f + (1.0f - 1.0e-9f) * rp;
+  }
+};
+
+enum ApplyMode : int {
+  kModeApply = 0,   // out = K u (identity on fixed DOFs)
+  kModeResid = 1,   // out = b - K u (0 on fixed DOFs)
+  kModeJacobi = 2,  // out = u + omega Dinv (b - K u) (0 on fixed DOFs)
+  kModeCgQ = 3,     // out = K u, partials += u . out
+};
+
+template <typename T, class ESrc>
+struct FineParams {
+  KEP<T> ke;
+  Grid g;          // element grid
+  int TY, TX, ZC;  // node tile and z chunk
+  int tiles_y, tiles_x;
+  const T* u;
+  const uint8_t* fix;  // per node, bit c = DOF c fixed
+  ESrc esrc;
+  T* out;
+  const T* b;
+  const T* dinv;
+  T omega;
+  double* partials;
+  const int* done;  // early-exit flag (may be null)
+};
+
+// Shared memory: 3 planes x 3 comps x (TX+2)(TY+2) of T, then 2 slabs x (TX+1)(TY+1) of T.
+template <typename T>
+__host__ __device__ inline size_t fine_smem_bytes(int TY, int TX) {
+  return (size_t)(9 * (TX + 2) * (TY + 2) + 2 * (TX + 1) * (TY + 1)) * sizeof(T);
+}
+
+template <typename T, int MODE, class ESrc>
+__global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__ FineParams<T, ESrc> p) {
+  if (p.done && *(volatile const int*)p.done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);
+  const int PY = p.TY + 2, PX = p.TX + 2, PP = PY * PX;
+  T* se = su + 9 * PP;
+  const int EY = p.TY + 1, EX = p.TX + 1, EP = EY * EX;
+  __shared__ double red[32];
+
+  const int NX = p.g.nx + 1, NY = p.g.ny + 1, NZ = p.g.nz + 1;
+  const int by = blockIdx.x % p.tiles_y;
+  const int bx = blockIdx.x / p.tiles_y;
+  const int x0 = bx * p.TX, y0 = by * p.TY;
+  const int zb = blockIdx.y * p.ZC;
+  const int ze = min(zb + p.ZC, NZ);
+  const int tid = threadIdx.x;
+  const int ty = tid % p.TY, tx = tid / p.TY;
+  const bool active = (tx < p.TX) && (x0 + tx < NX) && (y0 + ty < NY);
+
+  auto stage_plane = [&](int zp) {
+    const int slot = (zp + 3) % 3;
+    T* dst = su + slot * 3 * PP;
+    for (int i = tid; i < PP; i += blockDim.x) {
+      const int ly = i % PY, lx = i / PY;
+      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+      T v0 = T(0), v1 = T(0), v2 = T(0);
+      if (zp >= 0 && zp < NZ && gx >= 0 && gx < NX && gy >= 0 && gy < NY) {
+        const long long n = p.g.nidx(gx, gy, zp);
+        const int f = p.fix[n];
+        const T* un = p.u + 3 * n;
+        v0 = (f & 1) ? T(0) : un[0];
+        v1 = (f & 2) ? T(0) : un[1];
+        v2 = (f & 4) ? T(0) : un[2];
+      }
+      dst[i] = v0;
+      dst[PP + i] = v1;
+      dst[2 * PP + i] = v2;
+    }
+  };
+  auto stage_slab = [&](int zs) {
+    T* dst = se + ((zs + 2) % 2) * EP;
+    for (int i = tid; i < EP; i += blockDim.x) {
+      const int ly = i % EY, lx = i / EY;
+      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+      T v = T(0);
+      if (zs >= 0 && zs < p.g.nz && gx >= 0 && gx < p.g.nx && gy >= 0 && gy < p.g.ny)
+        v = (T)p.esrc(p.g.eidx(gx, gy, zs));
+      dst[i] = v;
+    }
+  };
+
+  double part = 0.0;
+  stage_plane(zb - 1);
+  stage_plane(zb);
+  stage_slab(zb - 1);
+  for (int z = zb; z < ze; ++z) {
+    stage_plane(z + 1);
+    stage_slab(z);
+    __syncthreads();
+    if (active) {
+      T acc[8][3];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[e][c] = T(0);
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const T* pl = su + ((z + dz + 3) % 3) * 3 * PP;
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+#pragma unroll
+          for (int dy = -1; dy <= 1; ++dy) {
+            const int off = (tx + 1 + dx) * PY + (ty + 1 + dy);
+            const T um0 = pl[off], um1 = pl[PP + off], um2 = pl[2 * PP + off];
+#pragma unroll
+            for (int ez = -1; ez <= 0; ++ez)
+#pragma unroll
+              for (int ex = -1; ex <= 0; ++ex)
+#pragma unroll
+                for (int ey = -1; ey <= 0; ++ey) {
+                  const int ox = dx - ex, oy = dy - ey, oz = dz - ez;
+                  if (ox < 0 || ox > 1 || oy < 0 || oy > 1 || oz < 0 || oz > 1) continue;
+                  const int a = corner_index(-ex, -ey, -ez);
+                  const int b = corner_index(ox, oy, oz);
+                  const int e8 = (ez + 1) * 4 + (ey + 1) * 2 + (ex + 1);
+#pragma unroll
+                  for (int c = 0; c < 3; ++c) {
+                    T t = acc[e8][c];
+                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 0], um0, t);
+                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 1], um1, t);
+                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 2], um2, t);
+                    acc[e8][c] = t;
+                  }
+                }
+          }
+        }
+      }
+      T kv[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int ez = -1; ez <= 0; ++ez) {
+        const T* sl = se + ((z + ez + 2) % 2) * EP;
+#pragma unroll
+        for (int ex = -1; ex <= 0; ++ex)
+#pragma unroll
+          for (int ey = -1; ey <= 0; ++ey) {
+            const T E = sl[(tx + 1 + ex) * EY + (ty + 1 + ey)];
+            const int e8 = (ez + 1) * 4 + (ey + 1) * 2 + (ex + 1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) kv[c] = fma(E, acc[e8][c], kv[c]);
+          }
+      }
+      const long long n = p.g.nidx(x0 + tx, y0 + ty, z);
+      const int f = p.fix[n];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const bool fx = (f >> c) & 1;
+        const long long i = 3 * n + c;
+        if (MODE == kModeApply) {
+          p.out[i] = fx ? p.u[i] : kv[c];
+        } else if (MODE == kModeResid) {
+          p.out[i] = fx ? T(0) : p.b[i] - kv[c];
+        } else if (MODE == kModeJacobi) {
+          const T own = su[((z + 3) % 3) * 3 * PP + c * PP + (tx + 1) * PY + (ty + 1)];
+          p.out[i] = fx ? T(0) : own + p.omega * p.dinv[i] * (p.b[i] - kv[c]);
+        } else {  // kModeCgQ
+          const T own = su[((z + 3) % 3) * 3 * PP + c * PP + (tx + 1) * PY + (ty + 1)];
+          const T q = fx ? T(0) : kv[c];
+          p.out[i] = q;
+          part += (double)own * (double)q;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (MODE == kModeCgQ) {
+    part = block_sum(part, red);
+    if (tid == 0) p.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
+  }
+}
+
+// Diagonal of the fine operator: D[n,c] = sum_e E_e KE[3a+c][3a+c]; 1 on fixed DOFs.
+// Writes its inverse.
+template <typename T, class ESrc>
+__global__ void fine_diag_inv_kernel(Grid g, const __grid_constant__ KEP<double> ke, ESrc esrc,
+                                     const uint8_t* __restrict__ fix, T* dinv) {
+  const int NX = g.nx + 1, NY = g.ny + 1;
+  const long long nn = g.nnode();
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(n % NY);
+    const long long r = n / NY;
+    const int ix = (int)(r % NX), iz = (int)(r / NX);
+    double d[3] = {0, 0, 0};
+#pragma unroll
+    for (int ez = -1; ez <= 0; ++ez)
+#pragma unroll
+      for (int ex = -1; ex <= 0; ++ex)
+#pragma unroll
+        for (int ey = -1; ey <= 0; ++ey) {
+          const int x = ix + ex, y = iy + ey, z = iz + ez;
+          if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+          const double E = (double)esrc(g.eidx(x, y, z));
+          const int a = corner_index(-ex, -ey, -ez);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) d[c] += E * ke.k[(3 * a + c) * 24 + 3 * a + c];
+        }
+    const int f = fix[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dinv[3 * n + c] = ((f >> c) & 1) || !(d[c] > 0.0) ? T(0) : (T)(1.0 / d[c]);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// 27-point block-stencil levels
+// ----------------------------------------------------------------------------
+// coefficient index k = (jrel * 3 + c) * 3 + d, jrel = (dz+1)*9 + (dx+1)*3 + (dy+1);
+// storage A[k * nn + node].
+__host__ __device__ constexpr int stencil_k(int jrel, int c, int d) { return (jrel * 3 + c) * 3 + d; }
+__host__ __device__ constexpr int jrel_of(int dx, int dy, int dz) { return (dz + 1) * 9 + (dx + 1) * 3 + (dy + 1); }
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) stencil_apply_kernel(Grid g, const T* __restrict__ A,
+                                                            const uint8_t* __restrict__ fix,
+                                                            const T* __restrict__ u, T* out, const T* b,
+                                                            const T* dinv, T omega, double* partials,
+                                                            const int* done) {
+  if (done && *(volatile const int*)done) return;
+  __shared__ double red[32];
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const long long nn = g.nnode();
+  double part = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(n % NY);
+    const long long r = n / NY;
+    const int ix = (int)(r % NX), iz = (int)(r / NX);
+    T kv[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int x = ix + dx, y = iy + dy, z = iz + dz;
+          if (x < 0 || x >= NX || y < 0 || y >= NY || z < 0 || z >= NZ) continue;
+          const long long m = g.nidx(x, y, z);
+          const int fm = fix[m];
+          const int jr = jrel_of(dx, dy, dz);
+          T um[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) um[d] = ((fm >> d) & 1) ? T(0) : __ldg(&u[3 * m + d]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) kv[c] = fma(__ldg(&A[(long long)stencil_k(jr, c, d) * nn + n]), um[d], kv[c]);
+        }
+    const int f = fix[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const bool fx = (f >> c) & 1;
+      const long long i = 3 * n + c;
+      if (MODE == kModeApply) {
+        out[i] = fx ? u[i] : kv[c];
+      } else if (MODE == kModeResid) {
+        out[i] = fx ? T(0) : b[i] - kv[c];
+      } else if (MODE == kModeJacobi) {
+        out[i] = fx ? T(0) : u[i] + omega * dinv[i] * (b[i] - kv[c]);
+      } else {
+        const T q = fx ? T(0) : kv[c];
+        out[i] = q;
+        part += (double)u[i] * (double)q;
+      }
+    }
+  }
+  if (MODE == kModeCgQ) {
+    part = block_sum(part, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+  }
+}
+
+template <typename T>
+__global__ void stencil_diag_inv_kernel(Grid g, const double* __restrict__ A, const uint8_t* __restrict__ fix,
+                                        T* dinv) {
+  const long long nn = g.nnode();
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    const int f = fix[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double d = A[(long long)stencil_k(13, c, c) * nn + n];
+      dinv[3 * n + c] = (((f >> c) & 1) || !(d > 0.0)) ? T(0) : (T)(1.0 / d);
+    }
+  }
+}
+
+// x = omega * dinv * b (first Jacobi sweep from a zero guess)
+template <typename T>
+__global__ void jacobi_zero_kernel(long long ndof, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
+                                   T* x, const int* done) {
+  if (done && *(volatile const int*)done) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x)
+    x[i] = omega * dinv[i] * b[i];
+}
+
+// ----------------------------------------------------------------------------
+// grid transfer (trilinear, vertex-centred coarsening by 2)
+// ----------------------------------------------------------------------------
+// coarse element grid of a fine element grid
+__host__ __device__ inline Grid coarse_grid(const Grid& f) {
+  return Grid{(f.nx + 1) / 2, (f.ny + 1) / 2, (f.nz + 1) / 2};
+}
+
+// b_c[I] = sum_i P[i,I] r_f[i], 0 on fixed coarse DOFs.
+template <typename T>
+__global__ void restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf, const uint8_t* __restrict__ fixc, T* bc,
+                                const int* done) {
+  if (done && *(volatile const int*)done) return;
+  const int FX = gf.nx + 1, FY = gf.ny + 1, FZ = gf.nz + 1;
+  const int CX = gc.nx + 1, CY = gc.ny + 1;
+  const long long nn = gc.nnode();
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    const int Iy = (int)(n % CY);
+    const long long r = n / CY;
+    const int Ix = (int)(r % CX), Iz = (int)(r / CX);
+    T s[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int x = 2 * Ix + dx, y = 2 * Iy + dy, z = 2 * Iz + dz;
+          if (x < 0 || x >= FX || y < 0 || y >= FY || z < 0 || z >= FZ) continue;
+          const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+          const long long m = gf.nidx(x, y, z);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s[c] = fma(w, rf[3 * m + c], s[c]);
+        }
+    const int f = fixc[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) bc[3 * n + c] = ((f >> c) & 1) ? T(0) : s[c];
+  }
+}
+
+// x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.
+template <typename T>
+__global__ void prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc, const uint8_t* __restrict__ fixf,
+                                   T* xf, const int* done) {
+  if (done && *(volatile const int*)done) return;
+  const int FX = gf.nx + 1, FY = gf.ny + 1;
+  const long long nn = gf.nnode();
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    const int iy = (int)(n % FY);
+    const long long r = n / FY;
+    const int ix = (int)(r % FX), iz = (int)(r / FX);
+    T s[3] = {T(0), T(0), T(0)};
+    const int nxp = (ix & 1) ? 2 : 1, nyp = (iy & 1) ? 2 : 1, nzp = (iz & 1) ? 2 : 1;
+    const T wx = (ix & 1) ? T(0.5) : T(1), wy = (iy & 1) ? T(0.5) : T(1), wz = (iz & 1) ? T(0.5) : T(1);
+    for (int a = 0; a < nzp; ++a)
+      for (int b = 0; b < nxp; ++b)
+        for (int c2 = 0; c2 < nyp; ++c2) {
+          const int Ix = (ix >> 1) + b, Iy = (iy >> 1) + c2, Iz = (iz >> 1) + a;
+          const long long m = gc.nidx(Ix, Iy, Iz);
+          const T w = wx * wy * wz;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s[c] = fma(w, xc[3 * m + c], s[c]);
+        }
+    const int f = fixf[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if (!((f >> c) & 1)) xf[3 * n + c] += s[c];
+  }
+}
+
+}  // namespace tp3d

@@ -1,0 +1,519 @@
+"""``top3d`` on the B200: drop-in for pytopo3d/core/optimizer.py.
+
+Same signature, defaults, validation messages, exception types, return tuple
+and ``diagnostics_out`` keys as the reference ``top3d`` (optimizer.py:283-839)
+and ``evaluate_fixed_geometry_metrics`` / ``_compliance`` (:54-279).  The loop
+body runs on the device with the design kept as flat Fortran-ordered CUDA
+vectors; the host sees two scalars per iteration (compliance and change)
+plus the logging metrics.
+
+Extensions (keyword-only): ``F`` — an explicit nodal load vector, or a 2-D
+array of load cases whose compliances are summed; ``precision`` — "fp64"
+(default) or "mixed"; ``solver_options`` — HexSolver options;
+``record`` — a list receiving per-iteration stats.
+"""
+
+from __future__ import annotations
+
+import logging
+import time
+from typing import Any, Dict, MutableMapping, Optional, Sequence, Tuple, Union
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._tensors import device, from_flat, to_flat, to_flat_mask, vec
+from .assembly import build_force_vector, build_supports
+from .filter import ConeFilter, build_filter, project_flat, transpose_flat
+from .oc_update import OCWorkspace, oc_update_flat
+from .solver import HexSolver
+from .stiffness import lk_H8
+
+logger = logging.getLogger(__name__)
+
+EMIN = 1.0e-9
+
+
+def _fixed_dof_mask(nelx, nely, nelz, support_mask):
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    free, _ = build_supports(nelx, nely, nelz, ndof, support_mask)
+    fixed = np.ones(ndof, dtype=np.uint8)
+    fixed[free] = 0
+    return fixed
+
+
+def _elements_at_loaded_nodes(F2, nelx, nely, nelz):
+    """Elements touching a loaded node: the explicit-load analogue of the default
+    load strip protection (optimizer.py:366-369)."""
+    loaded = np.any(F2.reshape(F2.shape[0], -1, 3) != 0.0, axis=(0, 2))
+    node = loaded.reshape(nelz + 1, nelx + 1, nely + 1)  # [iz, ix, iy]
+    el = np.zeros((nelz, nelx, nely), dtype=bool)
+    for oz in (0, 1):
+        for ox in (0, 1):
+            for oy in (0, 1):
+                el |= node[oz:oz + nelz, ox:ox + nelx, oy:oy + nely]
+    return el.transpose(2, 1, 0)
+
+
+def _ke(material_params, elem_size):
+    return lk_H8(elem_size=elem_size) if material_params is None else lk_H8(*material_params,
+                                                                              elem_size=elem_size)
+
+
+class SimpState:
+    """Device buffers of one SIMP loop: flat Fortran-ordered element vectors."""
+
+    def __init__(self, H: ConeFilter, Hs, solid, void, free, KE, F, solver: HexSolver, penal):
+        self.H, self.Hs = H, Hs
+        self.solid, self.void, self.free = solid, void, free
+        self.KE = np.ascontiguousarray(KE)
+        self.F = F  # (ncases, ndof)
+        self.solver = solver
+        self.penal = float(penal)
+        n = H.nelx * H.nely * H.nelz
+        z = lambda: torch.empty(n, dtype=torch.float64, device=device())
+        self.rho_f, self.rho_p, self.dproj = z(), z(), z()
+        self.x_new, self.rho_new = z(), z()
+        self.dc_dx, self.dv_dx, self.ce = z(), z(), z()
+        self.dc_acc = z()
+        self.c_dev = torch.zeros(2, dtype=torch.float64, device=device())
+        self.U = torch.zeros_like(F)
+        self.sens_scratch = torch.empty(
+            _lib.lib().tp3d_sensitivity_scratch_bytes(H.nelx, H.nely, H.nelz), dtype=torch.uint8,
+            device=device())
+        self.ws = OCWorkspace(H)
+
+    def project(self, x, beta, eta, rho_f=None, rho_p=None, dproj=None):
+        return project_flat(self.H, x, self.Hs, beta, eta, self.solid, self.void,
+                            self.rho_f if rho_f is None else rho_f,
+                            self.rho_p if rho_p is None else rho_p,
+                            self.dproj if dproj is None else dproj)
+
+    def sensitivities(self, rho_p, dproj):
+        """Solve every load case, then fused energy / compliance / chain rule."""
+        L = _lib.lib()
+        H = self.H
+        self.solver.set_density(rho_p, self.penal)
+        iters = 0
+        for k in range(self.F.shape[0]):
+            self.solver.solve(self.F[k], self.U[k])
+            iters += self.solver.last_iterations
+            dst_dc = self.dc_dx if k == 0 else self.dc_acc
+            _lib.check(L.tp3d_sensitivity(
+                H.nelx, H.nely, H.nelz, H.rmin, self.U[k].data_ptr(), self.KE.ctypes.data,
+                rho_p.data_ptr(), dproj.data_ptr(), self.Hs.data_ptr(), self.free.data_ptr(), self.penal,
+                self.ce.data_ptr(), dst_dc.data_ptr(), self.dv_dx.data_ptr(),
+                self.c_dev[min(k, 1)].data_ptr(), self.sens_scratch.data_ptr(), _lib.stream_ptr()),
+                "sensitivity")
+            if k > 0:
+                self.dc_dx += self.dc_acc
+                self.c_dev[0] += self.c_dev[1]
+        return iters
+
+
+class SimpLoop:
+    """Stateful SIMP loop on the device: set up once, then one ``step()`` per
+    iteration of the loop body (optimizer.py:578-696).
+
+    ``step()`` works on device-resident state; ``step_host(x)`` takes and
+    returns host arrays (pinned copies in both directions) for callers that keep
+    the design on the host.
+    """
+
+    def __init__(self, nelx, nely, nelz, volfrac, penal, rmin, KE, F, fixed_dofs, protected_solid,
+                 protected_void, projection_eta=0.5, move=0.2, precision="fp64", solver_options=None,
+                 x0=None):
+        self.shape = (nely, nelx, nelz)
+        solid = np.asarray(protected_solid, bool)
+        void = np.asarray(protected_void, bool)
+        free = ~(solid | void)
+        self.free_host = free
+        self.target = float(volfrac * int(free.sum()))
+        self.eta, self.move, self.penal = float(projection_eta), float(move), float(penal)
+        H, Hs = build_filter(nelx, nely, nelz, rmin)
+        self.solver = HexSolver(nelx, nely, nelz, KE, fixed_dofs, precision=precision,
+                                **(solver_options or {}))
+        Fd = torch.as_tensor(np.atleast_2d(np.asarray(F, dtype=np.float64))).to(device()).contiguous()
+        self.S = SimpState(H, Hs, to_flat_mask(solid), to_flat_mask(void), to_flat_mask(free), KE, Fd,
+                           self.solver, penal)
+        if x0 is None:
+            x0 = np.full(self.shape, volfrac, dtype=float)
+            x0[solid] = 1.0
+            x0[void] = 0.0
+        self.x = to_flat(x0)
+        self.beta = None
+        self.last = {}
+        n = self.x.numel()
+        self._pin_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        self._pin_out = torch.empty(n + 1, dtype=torch.float64, pin_memory=True)
+
+    def set_beta(self, beta):
+        self.beta = float(beta)
+        self.S.project(self.x, self.beta, self.eta)
+
+    def step(self):
+        """One loop body: solve, sensitivities, OC update, re-projection.
+        Returns the device stats tensor [c, lambda, volume, steps, change, ...]."""
+        S = self.S
+        cg = S.sensitivities(S.rho_p, S.dproj)
+        stats = oc_update_flat(S.H, self.x, S.dc_dx, S.dv_dx, S.Hs, S.solid, S.void, self.move, self.target,
+                               self.beta, self.eta, S.x_new, S.rho_new, S.ws)
+        self.x, S.x_new = S.x_new, self.x
+        S.project(self.x, self.beta, self.eta)
+        self.last = dict(cg_iterations=cg, relres=self.solver.last_relres)
+        return torch.cat([S.c_dev[:1], stats])
+
+    def step_host(self, x_host: np.ndarray):
+        """Host design in (Fortran-flat or (nely, nelx, nelz)), host (x_new, compliance) out."""
+        xf = np.asarray(x_host, dtype=np.float64)
+        if xf.ndim == 3:
+            xf = xf.transpose(2, 1, 0).reshape(-1)
+        self._pin_in.numpy()[:] = xf
+        self.x.copy_(self._pin_in, non_blocking=True)
+        self.S.project(self.x, self.beta, self.eta)
+        st = self.step()
+        self._pin_out[:-1].copy_(self.x, non_blocking=True)
+        self._pin_out[-1:].copy_(st[:1], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        out = self._pin_out.numpy()
+        return out[:-1].copy(), float(out[-1])
+
+    def design(self):
+        return from_flat(self.x, self.shape)
+
+    def physical(self):
+        return from_flat(self.S.rho_p, self.shape)
+
+    def close(self):
+        self.solver.close()
+
+
+def _free_stats(rho: torch.Tensor, free: torch.Tensor):
+    f = free.bool()
+    r = rho[f]
+    return float(r.mean()), float(((r > 0.05) & (r < 0.95)).double().mean())
+
+
+def top3d(
+    nelx: int,
+    nely: int,
+    nelz: int,
+    volfrac: float,
+    penal: float,
+    rmin: float,
+    disp_thres: float,
+    material_params: Optional[Sequence[float]] = None,
+    elem_size: float = 0.01,
+    obstacle_mask: Optional[np.ndarray] = None,
+    force_field: Optional[np.ndarray] = None,
+    support_mask: Optional[np.ndarray] = None,
+    tolx: float = 0.01,
+    maxloop: int = 2000,
+    save_history: bool = False,
+    history_frequency: int = 10,
+    use_gpu: bool = False,
+    protected_zone_mask: Optional[np.ndarray] = None,
+    beta_schedule: Sequence[float] = (1.0, 2.0, 4.0, 8.0),
+    projection_eta: float = 0.5,
+    move: float = 0.2,
+    diagnostics_out: Optional[MutableMapping[str, Any]] = None,
+    *,
+    F: Optional[np.ndarray] = None,
+    precision: str = "fp64",
+    solver_options: Optional[Dict[str, Any]] = None,
+    record: Optional[list] = None,
+) -> Tuple[np.ndarray, Optional[Dict[str, list]], float, None]:
+    """Density-filtered SIMP with Heaviside continuation (optimizer.py:283-839).
+
+    ``maxloop`` caps each beta stage.  Returns ``(xPhys, history, compliance,
+    None)`` with xPhys the projected physical density (numpy, (nely, nelx, nelz)).
+    ``use_gpu`` is accepted for signature compatibility; the path is always the B200.
+    """
+    # ---- validation (optimizer.py:313-341) ----
+    if min(nelx, nely, nelz) < 1:
+        raise ValueError("nelx, nely, and nelz must all be positive")
+    expected_shape = (nely, nelx, nelz)
+    if not 0.0 < volfrac <= 1.0:
+        raise ValueError(f"volfrac must be in (0, 1], got {volfrac}")
+    if not np.isfinite(penal) or penal <= 0:
+        raise ValueError(f"penal must be positive, got {penal}")
+    if not np.isfinite(maxloop) or maxloop < 1:
+        raise ValueError(f"maxloop must be at least 1, got {maxloop}")
+    if not np.isfinite(tolx) or tolx <= 0:
+        raise ValueError(f"tolx must be positive, got {tolx}")
+    if not np.isfinite(history_frequency) or history_frequency < 1:
+        raise ValueError(f"history_frequency must be at least 1, got {history_frequency}")
+    if not np.isfinite(move) or move <= 0:
+        raise ValueError(f"move must be positive, got {move}")
+    if not 0.0 < projection_eta < 1.0:
+        raise ValueError(f"projection_eta must be between 0 and 1, got {projection_eta}")
+    beta_schedule = tuple(float(b) for b in beta_schedule)
+    if not beta_schedule:
+        raise ValueError("beta_schedule must contain at least one value")
+    if any(not np.isfinite(b) or b <= 0.0 for b in beta_schedule):
+        raise ValueError(f"all beta_schedule values must be finite and positive, got {beta_schedule}")
+
+    # ---- masks (optimizer.py:346-405) ----
+    obstacle_mask = (np.zeros(expected_shape, dtype=bool) if obstacle_mask is None
+                     else np.asarray(obstacle_mask, dtype=bool).copy())
+    protected_zone_mask = (np.zeros(expected_shape, dtype=bool) if protected_zone_mask is None
+                           else np.asarray(protected_zone_mask, dtype=bool).copy())
+    if obstacle_mask.shape != expected_shape:
+        raise ValueError(f"obstacle_mask has shape {obstacle_mask.shape}, expected {expected_shape}")
+    if protected_zone_mask.shape != expected_shape:
+        raise ValueError("protected_zone_mask has shape "
+                         f"{protected_zone_mask.shape}, expected {expected_shape}")
+    if force_field is None:
+        if F is None:
+            protected_zone_mask[:, -1, 0] = True
+        else:
+            protected_zone_mask |= _elements_at_loaded_nodes(np.atleast_2d(F), nelx, nely, nelz)
+    else:
+        if force_field.shape != expected_shape + (3,):
+            raise ValueError(f"force_field has shape {force_field.shape}, "
+                             f"expected {expected_shape + (3,)}")
+        protected_zone_mask |= np.any(force_field != 0.0, axis=-1)
+    if support_mask is None:
+        protected_zone_mask[:, 0, :] = True
+    else:
+        if support_mask.shape != expected_shape:
+            raise ValueError(f"support_mask has shape {support_mask.shape}, expected {expected_shape}")
+        if np.any(support_mask):
+            protected_zone_mask |= np.asarray(support_mask, dtype=bool)
+        else:
+            protected_zone_mask[:, 0, :] = True
+    overlap = obstacle_mask & protected_zone_mask
+    if np.any(overlap):
+        logger.warning("Protected-solid and protected-void masks overlap at %d elements; "
+                       "protected void takes precedence.", int(np.sum(overlap)))
+        protected_zone_mask[overlap] = False
+    free_mask = ~(obstacle_mask | protected_zone_mask)
+    design_nele = int(np.sum(free_mask))
+    if design_nele == 0:
+        raise ValueError("optimization requires at least one free design element")
+    target_free_volume = float(volfrac * design_nele)
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+
+    # ---- setup (optimizer.py:427-463) on the device ----
+    if F is None:
+        Fh = build_force_vector(nelx, nely, nelz, ndof, force_field)[None, :]
+    else:
+        Fh = np.atleast_2d(np.asarray(F, dtype=np.float64))
+        if Fh.shape[1] != ndof:
+            raise ValueError(f"F must have {ndof} entries per load case")
+    KE = _ke(material_params, elem_size)
+    H, Hs = build_filter(nelx, nely, nelz, rmin)
+    solid, void, free = (to_flat_mask(protected_zone_mask), to_flat_mask(obstacle_mask),
+                         to_flat_mask(free_mask))
+    solver = HexSolver(nelx, nely, nelz, KE, _fixed_dof_mask(nelx, nely, nelz, support_mask),
+                       precision=precision, **(solver_options or {}))
+    Fd = torch.as_tensor(Fh, dtype=torch.float64).to(device()).contiguous()
+    S = SimpState(H, Hs, solid, void, free, KE, Fd, solver, penal)
+
+    x0 = np.full(expected_shape, volfrac, dtype=float)
+    x0[protected_zone_mask] = 1.0
+    x0[obstacle_mask] = 0.0
+    x = to_flat(x0)
+    history = ({"density_history": [], "iteration_history": [], "compliance_history": [],
+                "beta_history": []} if save_history else None)
+
+    def bounds(beta):
+        lo = np.zeros(expected_shape)
+        lo[protected_zone_mask] = 1.0
+        hi = np.ones(expected_shape)
+        hi[obstacle_mask] = 0.0
+        out = []
+        for d in (lo, hi):
+            _, rp, _ = S.project(to_flat(d), beta, projection_eta, torch.empty_like(x),
+                                 torch.empty_like(x), torch.empty_like(x))
+            out.append(float(rp[free.bool()].mean()))
+        return out
+
+    total_loop = 0
+    c = float("nan")
+    stage_summaries = []
+    for beta in beta_schedule:
+        logger.info("Starting projection stage: beta=%g", beta)
+        change, stage_loop, c_prev = float("inf"), 0, float("nan")
+        S.project(x, beta, projection_eta)
+        vmin, vmax = bounds(beta)
+        within = vmin - 1.0e-10 <= volfrac <= vmax + 1.0e-10
+        if volfrac < vmin - 1.0e-10:
+            raise ValueError(
+                "projected free-volume target is infeasible at "
+                f"beta={beta:g}: target={volfrac:.6f}, minimum achievable="
+                f"{vmin:.6f}. Protected-solid density "
+                "spreads into the free region through the density filter.")
+        if volfrac > vmax + 1.0e-10:
+            logger.warning("Projected free-volume target %.6f exceeds the maximum achievable %.6f at "
+                           "beta=%g; the volume upper bound is inactive at the all-solid free design.",
+                           volfrac, vmax, beta)
+        while change > tolx and stage_loop < maxloop:
+            stage_loop += 1
+            total_loop += 1
+            t0 = time.time()
+            rho_used = S.rho_p.clone() if save_history else None
+            cg_iters = S.sensitivities(S.rho_p, S.dproj)
+            stats = oc_update_flat(H, x, S.dc_dx, S.dv_dx, Hs, solid, void, move, target_free_volume, beta,
+                                   projection_eta, S.x_new, S.rho_new, S.ws)
+            host = torch.cat([S.c_dev[:1], stats]).cpu().numpy()
+            c, change = float(host[0]), float(host[4])
+            if not np.isfinite(host[3]):
+                raise _lib.Topo3dError("OC bisection did not finish (bounded device wait expired)")
+            x, S.x_new = S.x_new, x
+            c_delta = c - c_prev if np.isfinite(c_prev) else float("nan")
+            c_prev = c
+            if record is not None:
+                record.append(dict(beta=beta, c=c, change=change, cg_iterations=cg_iters,
+                                   relres=solver.last_relres, bisection_steps=int(host[3]),
+                                   lam=float(host[1])))
+            if save_history and ((total_loop - 1) % history_frequency == 0 or change <= tolx
+                                 or stage_loop == maxloop):
+                history["density_history"].append(from_flat(rho_used, expected_shape).cpu().numpy())
+                history["iteration_history"].append(total_loop - 1)
+                history["compliance_history"].append(c)
+                history["beta_history"].append(beta)
+            if logger.isEnabledFor(logging.INFO):
+                vol, gray = _free_stats(S.rho_new, free)
+                logger.info("beta=%4.1f iter=%4d total=%4d C=%.6e dC=%.3e vol=%.5f gray=%.5f "
+                            "change=%.5e time=%.2fs cg=%d", beta, stage_loop, total_loop, c, c_delta, vol,
+                            gray, change, time.time() - t0, cg_iters)
+            S.project(x, beta, projection_eta)
+        vol, gray = _free_stats(S.rho_p, free)
+        converged = change <= tolx
+        if not converged:
+            logger.warning("Projection stage beta=%g reached maxloop=%d without converging: final change "
+                           "%.6e exceeds tolx %.6e.", beta, maxloop, change, tolx)
+        stage_summaries.append({
+            "beta": float(beta), "iterations": int(stage_loop), "converged": bool(converged),
+            "physical_density_fraction": vol, "volume_fraction_error": vol - float(volfrac),
+            "gray_fraction_005_095": gray, "final_change": float(change),
+            "minimum_achievable_physical_fraction": vmin, "maximum_achievable_physical_fraction": vmax,
+            "target_within_achievable_range": within})
+
+    final_beta = beta_schedule[-1]
+    S.project(x, final_beta, projection_eta)
+    final_x = from_flat(x, expected_shape).cpu().numpy()
+    final_rho_filtered = from_flat(S.rho_f, expected_shape).cpu().numpy()
+    final_xPhys = from_flat(S.rho_p, expected_shape).cpu().numpy()
+
+    ev = dict(penal=penal, material_params=material_params, elem_size=elem_size, force_field=force_field,
+              support_mask=support_mask, obstacle_mask=obstacle_mask,
+              protected_zone_mask=protected_zone_mask, _solver=solver, _F=Fd)
+    final_compliance = evaluate_fixed_geometry_compliance(xPhys=final_xPhys, **ev)
+    if save_history:
+        history["density_history"].append(final_xPhys.copy())
+        history["iteration_history"].append(total_loop)
+        history["compliance_history"].append(float(final_compliance))
+        history["beta_history"].append(float(final_beta))
+    rho_binary = (final_xPhys >= 0.5).astype(float)
+    rho_binary[protected_zone_mask] = 1.0
+    rho_binary[obstacle_mask] = 0.0
+    binary_compliance = evaluate_fixed_geometry_compliance(xPhys=rho_binary, **ev)
+    delta = ((binary_compliance - final_compliance) / final_compliance if final_compliance != 0.0 else None)
+    fv = final_xPhys[free_mask]
+    gray_mask = (fv > 0.05) & (fv < 0.95)
+    metrics = {
+        "projection_enabled": True,
+        "projection_beta": float(final_beta),
+        "projection_beta_schedule": [float(b) for b in beta_schedule],
+        "projection_eta": float(projection_eta),
+        "penal": float(penal),
+        "design_variable_fraction": float(np.mean(final_x[free_mask])),
+        "filtered_density_fraction": float(np.mean(final_rho_filtered[free_mask])),
+        "physical_density_fraction": float(np.mean(fv)),
+        "gray_fraction_005_095": float(np.mean(gray_mask.astype(float))),
+        "projected_compliance": float(final_compliance),
+        "binary_compliance": float(binary_compliance),
+        "binary_compliance_delta": None if delta is None else float(delta),
+        "binary_threshold": 0.5,
+        "target_free_volume_fraction": float(volfrac),
+        "physical_volume_fraction_error": float(np.mean(fv) - volfrac),
+        "projection_total_iterations": int(total_loop),
+        "projection_stage_summaries": stage_summaries,
+        "projection_converged": all(s["converged"] for s in stage_summaries),
+        "projection_target_within_achievable_range": all(
+            s["target_within_achievable_range"] for s in stage_summaries),
+    }
+    logger.info("Final projection: beta=%.1f eta=%.3f vol=%.5f gray=%.5f C_projected=%.6e C_binary=%.6e",
+                final_beta, projection_eta, metrics["physical_density_fraction"],
+                metrics["gray_fraction_005_095"], final_compliance, binary_compliance)
+    if diagnostics_out is not None:
+        diagnostics_out.clear()
+        diagnostics_out.update(metrics)
+    solver.close()
+    return final_xPhys, history, final_compliance, None
+
+
+def evaluate_fixed_geometry_metrics(xPhys, penal, material_params=None, elem_size=0.01, force_field=None,
+                                    support_mask=None, obstacle_mask=None, protected_zone_mask=None,
+                                    use_gpu=False, *, F=None, precision="fp64", _solver=None, _F=None):
+    """One device solve on a fixed design plus load-patch metrics (optimizer.py:54-252)."""
+    xPhys = np.asarray(xPhys, dtype=float)
+    nely, nelx, nelz = xPhys.shape
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    x_eval = xPhys.copy()
+    if protected_zone_mask is not None:
+        x_eval[np.asarray(protected_zone_mask, bool)] = 1.0
+    if obstacle_mask is not None:
+        x_eval[np.asarray(obstacle_mask, bool)] = 0.0
+    if _F is not None:
+        Fd = _F
+        Fh = _F.cpu().numpy()
+    else:
+        Fh = (build_force_vector(nelx, nely, nelz, ndof, force_field) if F is None
+              else np.asarray(F, dtype=np.float64))
+        Fh = np.atleast_2d(Fh)
+        Fd = torch.as_tensor(Fh).to(device())
+    KE = _ke(material_params, elem_size)
+    solver = _solver
+    if solver is None:
+        solver = HexSolver(nelx, nely, nelz, KE, _fixed_dof_mask(nelx, nely, nelz, support_mask),
+                           precision=precision)
+    rho = to_flat(x_eval)
+    solver.set_density(rho, penal)
+    E = EMIN + (1.0 - EMIN) * rho ** penal
+    total = 0.0
+    U_all = []
+    ce = torch.empty_like(rho)
+    for k in range(Fd.shape[0]):
+        U = solver.solve(Fd[k])
+        _lib.check(_lib.lib().tp3d_element_compliance(nelx, nely, nelz, U.data_ptr(),
+                                                      np.ascontiguousarray(KE).ctypes.data, ce.data_ptr(),
+                                                      _lib.stream_ptr()), "element_compliance")
+        total += float(torch.dot(E, ce))
+        U_all.append(U)
+    U = U_all[0].cpu().numpy()
+    F0 = Fh[0]
+    loaded = np.flatnonzero(np.abs(F0) > 0.0)
+    nodes = np.unique(loaded // 3)
+    out = {"compliance": float(total)}
+    tot = {}
+    for ci, ax in enumerate("xyz"):
+        d = 3 * nodes + ci
+        tot[ax] = float(np.sum(np.abs(F0[d]))) if d.size else 0.0
+        out[f"u{ax}_avg_load_patch"] = float(np.mean(U[d])) if d.size else None
+    for ax in "xyz":
+        u = out[f"u{ax}_avg_load_patch"]
+        out[f"k_avg_{ax}"] = (float(tot[ax] / abs(u)) if u is not None and u != 0.0 and tot[ax] > 0.0
+                              else None)
+    dom = max((("x", tot["x"]), ("y", tot["y"]), ("z", tot["z"])), key=lambda t: t[1])[0]
+    out["k_avg"] = out[f"k_avg_{dom}"]
+    out["F_total"] = float(np.sum(np.abs(F0[loaded]))) if loaded.size else 0.0
+    for ax in "xyz":
+        out[f"F_total_{ax}"] = tot[ax]
+    for ax in "xyz":
+        out[f"loaded_{ax}_dof_count"] = int(nodes.size)
+    if _solver is None:
+        solver.close()
+    return out
+
+
+def evaluate_fixed_geometry_compliance(xPhys, penal, material_params=None, elem_size=0.01,
+                                       force_field=None, support_mask=None, obstacle_mask=None,
+                                       protected_zone_mask=None, use_gpu=False, **kw) -> float:
+    """Compliance only (optimizer.py:255-279)."""
+    return float(evaluate_fixed_geometry_metrics(xPhys, penal, material_params, elem_size, force_field,
+                                                 support_mask, obstacle_mask, protected_zone_mask, use_gpu,
+                                                 **kw)["compliance"])

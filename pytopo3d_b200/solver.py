@@ -1,0 +1,121 @@
+"""Matrix-free multigrid-preconditioned CG for K(rho) U = F on the B200.
+
+Replaces the reference's solve boundary: the per-iteration CSR assembly and
+``solver_func(Kff, F[free])`` from ``get_solver`` (pytopo3d/utils/solver.py:
+15-73, called at pytopo3d/core/optimizer.py:584-594).  Two forms:
+
+* ``precision="fp64"``: FP64 operator, FP64 multigrid V-cycle, PCG to the
+  relative residual ``rtol`` (default 1e-10);
+* ``precision="mixed"``: FP32 operator with BF16 densities, FP32 smoother and
+  CG vectors (FP64 dot products) inside FP64 iterative refinement whose
+  residual ``f - K u`` and update of ``u`` are FP64.
+
+Non-convergence raises ``RuntimeError`` like the reference's CuPy path
+(solver.py:57-58).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._tensors import device, vec
+
+DEFAULTS = dict(max_iterations=2000, rtol=1e-10, pre_sweeps=2, post_sweeps=2, omega=0.6,
+                coarsest_max_dofs=500, max_levels=12, inner_rtol=1e-4, max_refinements=30)
+
+
+class HexSolver:
+    """Solver handle for one grid, one support set and one stream."""
+
+    def __init__(self, nelx: int, nely: int, nelz: int, KE, fixed_dofs, precision: str = "fp64",
+                 **opts):
+        self.grid = (int(nelx), int(nely), int(nelz))
+        self.ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+        self.nele = nelx * nely * nelz
+        self.precision = precision
+        L = _lib.lib()
+        o = _lib.SolverOpts()
+        L.tp3d_solver_default_opts(C.byref(o))
+        o.precision = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown solver option {k}")
+            setattr(o, k, v)
+        self.opts = o
+        self.KE = np.ascontiguousarray(np.asarray(KE, dtype=np.float64))
+        if self.KE.shape != (24, 24):
+            raise ValueError("KE must be 24x24")
+        fx = torch.as_tensor(np.asarray(fixed_dofs) if isinstance(fixed_dofs, np.ndarray) else fixed_dofs)
+        fx = fx.to(device=device(), dtype=torch.uint8).contiguous()
+        if fx.numel() != self.ndof:
+            raise ValueError(f"fixed_dofs must have {self.ndof} entries")
+        self.fixed = fx
+        h = C.c_void_p()
+        _lib.check(L.tp3d_solver_create(nelx, nely, nelz, self.KE.ctypes.data, fx.data_ptr(), C.byref(o),
+                                        _lib.stream_ptr(), C.byref(h)), "tp3d_solver_create")
+        self._h = h
+        self.last_iterations = 0
+        self.last_relres = float("nan")
+
+    @classmethod
+    def from_freedofs(cls, nelx, nely, nelz, KE, freedofs, **kw):
+        ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+        fixed = np.ones(ndof, dtype=np.uint8)
+        fixed[np.asarray(freedofs, dtype=np.int64)] = 0
+        return cls(nelx, nely, nelz, KE, fixed, **kw)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().tp3d_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_density(self, rho_flat: torch.Tensor, penal: float):
+        """Moduli E = 1e-9 + (1 - 1e-9) rho^penal and the multigrid hierarchy."""
+        self._rho = rho_flat  # keep alive while the handle may read it
+        _lib.check(_lib.lib().tp3d_solver_set_density(self._h, rho_flat.data_ptr(), float(penal)),
+                   "set_density")
+
+    def solve(self, F: torch.Tensor, U: Optional[torch.Tensor] = None, raise_on_fail: bool = True):
+        """U (warm start if given, updated in place) solving K U = F on the free DOFs."""
+        F = vec(F)
+        U = torch.zeros_like(F) if U is None else U
+        it, rr = C.c_int(0), C.c_double(0)
+        rc = _lib.check(_lib.lib().tp3d_solver_solve(self._h, F.data_ptr(), U.data_ptr(), C.byref(it),
+                                                     C.byref(rr)), "solve")
+        self.last_iterations, self.last_relres = it.value, rr.value
+        if rc == _lib.TP3D_NOT_CONVERGED and raise_on_fail:
+            raise RuntimeError(f"CG failed to converge: iterations={it.value}, relres={rr.value:.3e}")
+        return U
+
+    def apply(self, u: torch.Tensor) -> torch.Tensor:
+        y = torch.empty_like(u)
+        fn = _lib.lib().tp3d_solver_apply_f64 if u.dtype == torch.float64 else _lib.lib().tp3d_solver_apply_f32
+        _lib.check(fn(self._h, u.data_ptr(), y.data_ptr()), "apply")
+        return y
+
+    def stats(self) -> dict:
+        buf = (C.c_double * 16)()
+        n = _lib.lib().tp3d_solver_stats(self._h, buf, 16)
+        keys = ["levels", "iterations", "refinements", "relres", "inner_iterations", "coarsest_dofs",
+                "tile_y", "tile_x", "z_chunk"]
+        return {k: buf[i] for i, k in enumerate(keys[:n])}
+
+
+def get_solver(use_gpu: bool = True):
+    """``(solver_factory, name)`` — the B200 counterpart of solver.py:69-73.
+
+    The reference returns a function of an assembled matrix; the B200 path is
+    matrix-free, so the factory returned here builds a :class:`HexSolver`.
+    """
+    return HexSolver, "B200 matrix-free multigrid PCG"

@@ -1,0 +1,161 @@
+"""Matrix-free operator and multigrid PCG against the oracle's assembled CSR K and spsolve.
+
+Tolerances: apply FP64 1e-13 relative to max|y|; apply FP32 2e-6; FP64 solve to
+relative residual 1e-10 compared with spsolve at 1e-8 (displacement) and
+1e-9 (compliance); mixed-precision compliance within 1e-6 of FP64.
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+import torch
+
+from oracle import simp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def P():
+    import pytopo3d_b200 as P
+    from pytopo3d_b200 import _lib
+
+    _lib.lib()
+    return P
+
+
+def _problem(nx, ny, nz, seed=0, support_mask=None, lo=0.0):
+    rng = np.random.default_rng(seed)
+    shape = (ny, nx, nz)
+    rho = rng.uniform(lo, 1.0, size=shape)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    free, fixed = O.build_supports(nx, ny, nz, ndof, support_mask)
+    fmask = np.ones(ndof, np.uint8)
+    fmask[free] = 0
+    return rho, free, fmask
+
+
+def _oracle_apply(rho, KE, penal, nx, ny, nz, fmask, u):
+    K, _ = O.assemble_K(rho, KE, penal, nx, ny, nz)
+    z = 1.0 - fmask
+    return z * (K @ (z * u)) + fmask * u
+
+
+@pytest.mark.parametrize("dims", [(6, 4, 3), (5, 7, 2), (1, 1, 1), (13, 3, 4), (8, 33, 3)])
+def test_apply_matches_assembled_matrix(P, dims):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=nx)
+    u = np.random.default_rng(1).normal(size=fmask.size)
+    y_ref = _oracle_apply(rho, KE, 3.0, nx, ny, nz, fmask, u)
+    for prec in ("fp64", "mixed"):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec)
+        s.set_density(to_flat(rho), 3.0)
+        y = s.apply(torch.as_tensor(u).cuda()).cpu().numpy()
+        np.testing.assert_allclose(y, y_ref, rtol=0, atol=1e-13 * np.abs(y_ref).max())
+        if prec == "mixed":
+            # BF16 densities: compare with the operator of the rounded densities
+            rho16 = torch.as_tensor(rho).to(torch.bfloat16).double().numpy()
+            y16_ref = _oracle_apply(rho16, KE, 3.0, nx, ny, nz, fmask, u.astype(np.float32).astype(float))
+            y32 = s.apply(torch.as_tensor(u, dtype=torch.float32).cuda()).double().cpu().numpy()
+            np.testing.assert_allclose(y32, y16_ref, rtol=0, atol=2e-6 * np.abs(y16_ref).max())
+        s.close()
+
+
+@pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
+def test_fp64_solve_matches_reference_direct_solve(P, golden, tag):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = (int(v) for v in golden[f"it{tag}_dims"][:3])
+    KE = P.lk_H8(elem_size=1.0)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    F = O.build_force_vector(nx, ny, nz, ndof)
+    free, _ = O.build_supports(nx, ny, nz, ndof)
+    s = HexSolver.from_freedofs(nx, ny, nz, KE, free, precision="fp64")
+    s.set_density(to_flat(golden[f"it{tag}_rho_p"]), 3.0)
+    U = s.solve(torch.as_tensor(F).cuda()).cpu().numpy()
+    Uref = golden[f"it{tag}_U"]
+    assert s.last_relres <= 1e-10
+    np.testing.assert_allclose(U, Uref, rtol=0, atol=1e-8 * np.abs(Uref).max())
+    assert F @ U == pytest.approx(F @ Uref, rel=1e-9)
+    s.close()
+
+
+@pytest.mark.parametrize("dims", [(16, 8, 8), (24, 12, 12), (20, 7, 9)])
+def test_mixed_precision_matches_fp64(P, dims):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=2, lo=0.0)
+    rho[rho < 0.3] = 0.0  # void pockets: E = 1e-9
+    ndof = fmask.size
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, ndof)).cuda()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(F)
+        assert s.last_relres <= 1e-10
+        out[prec] = U.cpu().numpy()
+        s.close()
+    Fh = F.cpu().numpy()
+    c64, c32 = Fh @ out["fp64"], Fh @ out["mixed"]
+    assert abs(c32 - c64) <= 1e-6 * abs(c64)
+    assert np.linalg.norm(out["mixed"] - out["fp64"]) <= 1e-6 * np.linalg.norm(out["fp64"])
+
+
+def test_multigrid_and_jacobi_agree_with_spsolve(P):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 10, 5, 6
+    KE = P.lk_H8(elem_size=0.01)
+    sm = np.zeros((ny, nx, nz), bool)
+    sm[1:3, 0, 2:4] = True  # small clamp patch: coarse levels need the dilation rule
+    rho, free, fmask = _problem(nx, ny, nz, seed=4, support_mask=sm, lo=0.05)
+    ndof = fmask.size
+    F = O.build_force_vector(nx, ny, nz, ndof)
+    Uref, _ = O.solve_displacement(rho, KE, 3.0, F, free, nx, ny, nz)
+    for opts in (dict(), dict(max_levels=1, max_iterations=20000)):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision="fp64", **opts)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(torch.as_tensor(F).cuda()).cpu().numpy()
+        np.testing.assert_allclose(U, Uref, rtol=0, atol=1e-7 * np.abs(Uref).max())
+        s.close()
+
+
+def test_iteration_cap_raises_runtime_error(P):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 12, 6, 6
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=6, lo=0.01)
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    s = HexSolver(nx, ny, nz, KE, fmask, precision="fp64", max_iterations=1)
+    s.set_density(to_flat(rho), 3.0)
+    with pytest.raises(RuntimeError, match="converge"):
+        s.solve(F)
+    s.close()
+
+
+def test_nonfinite_density_reports_an_error_not_a_hang(P):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 8, 4, 4
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=7, lo=0.1)
+    rho[1, 2, 1] = np.nan
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    s = HexSolver(nx, ny, nz, KE, fmask, precision="fp64", max_iterations=50)
+    s.set_density(to_flat(rho), 3.0)
+    with pytest.raises(RuntimeError):
+        s.solve(F)
+    s.close()

@@ -1,0 +1,172 @@
+"""The B200 SIMP loop against the reference's loop body and full top3d runs.
+
+Per-iteration parity from identical inputs (loop body of optimizer.py:584-642):
+densities 1e-12, U 1e-8 of max|U| (solver rtol 1e-10 vs direct solve),
+compliance 1e-9, new design 1e-8.  Whole runs: 1e-6 (OC decisions on a
+trajectory amplify round-off).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import simp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def P():
+    import pytopo3d_b200 as P
+    from pytopo3d_b200 import _lib
+
+    _lib.lib()
+    return P
+
+
+@pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
+def test_loop_body_matches_reference(P, golden, tag):
+    from pytopo3d_b200._tensors import from_flat, to_flat, to_flat_mask
+    from pytopo3d_b200.oc_update import oc_update_flat
+    from pytopo3d_b200.optimizer import SimpState, _fixed_dof_mask
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz, volfrac, penal, rmin, beta, eta, move, _ = golden[f"it{tag}_dims"]
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    shape = (ny, nx, nz)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    x, solid, void = golden[f"it{tag}_x"], golden[f"it{tag}_solid"], golden[f"it{tag}_void"]
+    free = ~(solid | void)
+    KE = P.lk_H8(elem_size=1.0)
+    H, Hs = P.build_filter(nx, ny, nz, rmin)
+    sd, vd, fd = to_flat_mask(solid), to_flat_mask(void), to_flat_mask(free)
+    solver = HexSolver(nx, ny, nz, KE, _fixed_dof_mask(nx, ny, nz, None))
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, ndof)[None]).cuda()
+    S = SimpState(H, Hs, sd, vd, fd, KE, F, solver, penal)
+    xd = to_flat(x)
+    S.project(xd, beta, eta)
+    np.testing.assert_allclose(from_flat(S.rho_p, shape).cpu().numpy(), golden[f"it{tag}_rho_p"], rtol=1e-12,
+                               atol=1e-13)
+    S.sensitivities(S.rho_p, S.dproj)
+    Uref = golden[f"it{tag}_U"]
+    np.testing.assert_allclose(S.U[0].cpu().numpy(), Uref, rtol=0, atol=1e-8 * np.abs(Uref).max())
+    assert float(S.c_dev[0]) == pytest.approx(float(golden[f"it{tag}_c"]), rel=1e-9)
+    dref = golden[f"it{tag}_dc_dx"]
+    np.testing.assert_allclose(from_flat(S.dc_dx, shape).cpu().numpy(), dref, rtol=0,
+                               atol=1e-8 * np.abs(dref).max())
+    oc_update_flat(H, xd, S.dc_dx, S.dv_dx, Hs, sd, vd, move, float(golden[f"it{tag}_target"]), beta, eta,
+                   S.x_new, S.rho_new, S.ws)
+    np.testing.assert_allclose(from_flat(S.x_new, shape).cpu().numpy(), golden[f"it{tag}_x_new"], rtol=0,
+                               atol=1e-8)
+    np.testing.assert_allclose(from_flat(S.rho_new, shape).cpu().numpy(), golden[f"it{tag}_rho_new"], rtol=0,
+                               atol=1e-8)
+    solver.close()
+
+
+def test_top3d_run_matches_reference(P, golden):
+    diag = {}
+    xphys, hist, comp, failure = P.top3d(nelx=6, nely=3, nelz=3, volfrac=0.4, penal=3.0, rmin=1.5,
+                                         disp_thres=0.5, elem_size=1.0, tolx=0.01, maxloop=4,
+                                         beta_schedule=(1.0, 2.0), save_history=True, history_frequency=1,
+                                         diagnostics_out=diag)
+    assert failure is None
+    np.testing.assert_allclose(xphys, golden["top3d_xphys"], rtol=0, atol=1e-6)
+    assert comp == pytest.approx(float(golden["top3d_compliance"]), rel=1e-6)
+    np.testing.assert_allclose(hist["compliance_history"], golden["top3d_hist_c"], rtol=1e-6)
+    assert diag["binary_compliance"] == pytest.approx(float(golden["top3d_binary_compliance"]), rel=1e-6)
+    assert diag["projection_total_iterations"] == int(golden["top3d_total_iterations"])
+
+
+def test_top3d_matches_oracle_trajectory(P):
+    rec = []
+    x, rho, hist = O.top3d(12, 6, 6, 0.3, 3.0, 2.0, tolx=0.01, maxloop=6, beta_schedule=(1.0, 2.0))
+    xphys, _, comp, _ = P.top3d(nelx=12, nely=6, nelz=6, volfrac=0.3, penal=3.0, rmin=2.0, disp_thres=0.5,
+                                elem_size=1.0, tolx=0.01, maxloop=6, beta_schedule=(1.0, 2.0), record=rec)
+    np.testing.assert_allclose([r["c"] for r in rec], hist, rtol=1e-7)
+    np.testing.assert_allclose(xphys, rho, rtol=0, atol=1e-6)
+
+
+def test_continuation_returns_one_physical_field_and_records_metrics(P):
+    # mirrors tests/test_projected_optimizer.py:184-249 of the reference
+    n = 2
+    shape = (n, n, n)
+    support = np.zeros(shape, bool)
+    support[:, 0, :] = True
+    ff = np.zeros(shape + (3,))
+    ff[0, 1, 0, 0] = 1.0
+    obstacle = np.zeros(shape, bool)
+    obstacle[1, 1, 1] = True
+    diag = {}
+    rho, history, comp, _ = P.top3d(nelx=n, nely=n, nelz=n, volfrac=0.5, penal=3.0, rmin=1.0, disp_thres=0.5,
+                                    force_field=ff, support_mask=support, obstacle_mask=obstacle, tolx=1e-12,
+                                    maxloop=1, save_history=True, history_frequency=1, beta_schedule=(1.0, 2.0),
+                                    diagnostics_out=diag)
+    prot = support | np.any(ff != 0.0, axis=-1)
+    assert np.all(rho[prot] == 1.0)
+    assert rho[obstacle].item() == 0.0
+    np.testing.assert_allclose(history["density_history"][-1], rho)
+    assert history["iteration_history"] == [0, 1, 2]
+    assert history["beta_history"] == [1.0, 2.0, 2.0]
+    assert history["compliance_history"][-1] == pytest.approx(comp)
+    for d, c in zip(history["density_history"], history["compliance_history"]):
+        rc = P.evaluate_fixed_geometry_compliance(xPhys=d, penal=3.0, force_field=ff, support_mask=support,
+                                                  obstacle_mask=obstacle)
+        assert c == pytest.approx(rc, rel=1e-9)
+    assert diag["projection_beta_schedule"] == [1.0, 2.0]
+    assert diag["projection_total_iterations"] == 2
+    assert diag["projection_converged"] is False
+    for st in diag["projection_stage_summaries"]:
+        assert st["volume_fraction_error"] == pytest.approx(0.0, abs=1e-7)
+    assert diag["physical_density_fraction"] == pytest.approx(0.5, abs=1e-7)
+
+
+def test_default_boundary_attachments_are_protected(P):
+    nx, ny, nz = 3, 2, 2
+    diag = {}
+    rho, _, _, _ = P.top3d(nelx=nx, nely=ny, nelz=nz, volfrac=0.5, penal=3.0, rmin=1.5, disp_thres=0.5,
+                           support_mask=np.zeros((ny, nx, nz), bool), maxloop=1, beta_schedule=(1.0,),
+                           diagnostics_out=diag)
+    assert np.all(rho[:, 0, :] == 1.0) and np.all(rho[:, -1, 0] == 1.0)
+    st = diag["projection_stage_summaries"][0]
+    assert st["minimum_achievable_physical_fraction"] > 0.0 and st["target_within_achievable_range"] is True
+    assert diag["physical_density_fraction"] == pytest.approx(0.5, abs=1e-7)
+
+
+def test_infeasible_target_is_reported_before_fea(P):
+    with pytest.raises(ValueError, match="minimum achievable"):
+        P.top3d(nelx=2, nely=2, nelz=2, volfrac=0.3, penal=3.0, rmin=1.5, disp_thres=0.5, maxloop=1,
+                beta_schedule=(1.0,))
+
+
+def test_symmetric_tensile_update_preserves_symmetry(P):
+    nx, ny, nz = 4, 12, 2
+    ff = P.build_force_field(nx, ny, nz, 0, nx, ny - 1, ny, 0, nz, 0.0, 1.0, 0.0)
+    sm = P.build_support_mask(nx, ny, nz, 0, nx, 0, 1, 0, nz)
+    prot = np.zeros((ny, nx, nz), bool)
+    prot[:3] = True
+    prot[-3:] = True
+    rho, _, _, _ = P.top3d(nelx=nx, nely=ny, nelz=nz, volfrac=0.5, penal=3.0, rmin=2.0, disp_thres=0.5,
+                           force_field=ff, support_mask=sm, protected_zone_mask=prot, tolx=1e-12, maxloop=1,
+                           beta_schedule=(1.0,))
+    f = rho[3:-3]
+    np.testing.assert_allclose(f, f[::-1], rtol=0, atol=1e-3)
+
+
+def test_fixed_geometry_metrics_match_reference(P, golden):
+    m = P.evaluate_fixed_geometry_metrics(golden["top3d_xphys"], 3.0, elem_size=1.0)
+    for k, v in m.items():
+        ref = float(golden[f"metrics_{k}"])
+        if v is None:
+            assert np.isnan(ref), k
+        else:
+            assert v == pytest.approx(ref, rel=1e-8, abs=1e-8 * abs(m["uz_avg_load_patch"])), k
+
+
+def test_mixed_precision_top3d_tracks_fp64(P):
+    kw = dict(nelx=24, nely=12, nelz=12, volfrac=0.3, penal=3.0, rmin=2.0, disp_thres=0.5, elem_size=1.0,
+              tolx=1e-9, maxloop=5, beta_schedule=(1.0,))
+    r64, r32 = [], []
+    x64, _, c64, _ = P.top3d(**kw, record=r64)
+    x32, _, c32, _ = P.top3d(**kw, record=r32, precision="mixed")
+    assert abs(r32[0]["c"] - r64[0]["c"]) <= 1e-6 * abs(r64[0]["c"])
+    assert abs(c32 - c64) <= 1e-5 * abs(c64)
