@@ -117,7 +117,7 @@ def make_loop(precision, x0=None):
     from pytopo3d_b200.optimizer import SimpLoop
     from pytopo3d_b200.stiffness import lk_H8
 
-    shape, solid, void, F, fixed = workload()
+    shape, solid, void, F, fixed = workload(NELX, NELY, NELZ)
     loop = SimpLoop(NELX, NELY, NELZ, VOLFRAC, PENAL, RMIN, lk_H8(elem_size=1.0), F, fixed, solid, void,
                     projection_eta=ETA, move=MOVE, precision=precision, x0=x0)
     loop.set_beta(BETA)
@@ -224,7 +224,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply"],
+                    help="step: warm-up + --steps loop bodies only (for launch lists); "
+                         "apply: fine-operator launches only (for kernel captures)")
+    ap.add_argument("--size", type=int, default=NELX, help="nelx for --mode step/apply (nely = nelz = nelx/2)")
     args = ap.parse_args()
+    if args.mode != "bench":
+        return run_probe(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -343,6 +349,32 @@ def main():
     loop.close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def run_probe(args):
+    """Small fixed workloads for profiler captures (no timing printed as a bench value)."""
+    global NELX, NELY, NELZ
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    NELX, NELY, NELZ = args.size, args.size // 2, args.size // 2
+    loop = make_loop(args.precision)
+    if args.mode == "step":
+        for _ in range(max(1, args.warmup)):
+            loop.step()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            loop.step()
+        torch.cuda.synchronize()
+        print(json.dumps({"mode": "step", "size": [NELX, NELY, NELZ], "steps": args.steps,
+                          "solver": loop.solver.stats()}))
+    else:
+        loop.step()
+        ms = ctypes_time_apply(loop.solver, fp32=(args.precision == "mixed"))
+        print(json.dumps({"mode": "apply", "size": [NELX, NELY, NELZ], "precision": args.precision,
+                          "apply_ms": ms}))
+    loop.close()
     return 0
 
 

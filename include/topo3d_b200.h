@@ -120,15 +120,19 @@ typedef struct tp3d_solver tp3d_solver;
 
 typedef struct tp3d_solver_opts {
   int precision;        /* TP3D_PRECISION_FP64 or TP3D_PRECISION_MIXED */
-  int max_iterations;   /* PCG iterations (FP64) / inner iterations per refinement step */
-  double rtol;          /* target ||f - K u|| / ||f|| */
-  int pre_sweeps;       /* smoother sweeps before restriction */
-  int post_sweeps;      /* smoother sweeps after prolongation */
-  double omega;         /* damped-Jacobi weight (<=0: Chebyshev) */
+  int max_iterations;   /* CG iterations */
+  double rtol;          /* target ||f - K u|| / ||f|| (checked on the FP64 residual) */
+  int pre_sweeps;       /* smoother degree before restriction (<= 8) */
+  int post_sweeps;      /* smoother degree after prolongation (<= 8) */
+  double omega;         /* damped-Jacobi weight when smoother == 1 */
   int coarsest_max_dofs;/* stop coarsening at or below this many DOFs */
   int max_levels;       /* cap on multigrid levels (1 = Jacobi-PCG only) */
-  double inner_rtol;    /* mixed: inner FP32 PCG tolerance per refinement step */
-  int max_refinements;  /* mixed: cap on FP64 refinement steps */
+  int smoother;         /* 0 Chebyshev(Jacobi) with power-iteration bounds, 1 damped Jacobi */
+  double cheb_ratio;    /* Chebyshev interval [lambda_max / ratio, lambda_max] */
+  int power_iterations; /* power iterations per level for lambda_max(Dinv A) */
+  int inner_density;    /* mixed: FP32 fine operator from 0 = FP32 moduli, 1 = BF16 densities */
+  double reliable_delta;/* mixed: replace the FP32 residual by the FP64 one when it fell by this factor */
+  int max_restarts;     /* FP64: restarts from the true residual when the recursive one drifted */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

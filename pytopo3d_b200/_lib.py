@@ -41,8 +41,12 @@ class SolverOpts(C.Structure):
         ("omega", f64),
         ("coarsest_max_dofs", i32),
         ("max_levels", i32),
-        ("inner_rtol", f64),
-        ("max_refinements", i32),
+        ("smoother", i32),
+        ("cheb_ratio", f64),
+        ("power_iterations", i32),
+        ("inner_density", i32),
+        ("reliable_delta", f64),
+        ("max_restarts", i32),
     ]
 
 

@@ -44,12 +44,68 @@ struct EFromBF16 {
   }
 };
 
-enum ApplyMode : int {
-  kModeApply = 0,   // out = K u (identity on fixed DOFs)
-  kModeResid = 1,   // out = b - K u (0 on fixed DOFs)
-  kModeJacobi = 2,  // out = u + omega Dinv (b - K u) (0 on fixed DOFs)
-  kModeCgQ = 3,     // out = K u, partials += u . out
+struct EFromF32 {
+  const float* E;
+  __device__ __forceinline__ float operator()(long long e) const { return __ldg(&E[e]); }
 };
+
+enum ApplyMode : int {
+  kModeApply = 0,      // out = K u (identity on fixed DOFs)
+  kModeResid = 1,      // out = b - K u (0 on fixed DOFs)
+  kModeJacobi = 2,     // out = u + omega Dinv (b - K u)
+  kModeCgQ = 3,        // out = K u, partials += u . out
+  kModeChebFirst = 4,  // d = c0 Dinv (b - K u); out = u + d
+  kModeChebStep = 5,   // d = c1 d + c2 Dinv (b - K u); out = u + d
+  kModeDinvApply = 6,  // out = Dinv K u (power iteration for lambda_max(Dinv K))
+};
+
+// Inputs / outputs shared by every operator kernel.
+template <typename T>
+struct OpIO {
+  const T* u = nullptr;
+  T* out = nullptr;
+  const T* b = nullptr;
+  const T* dinv = nullptr;
+  T* d = nullptr;                // Chebyshev direction (read-modify-write at own DOF)
+  const double* coef = nullptr;  // Chebyshev coefficients [c0, -, c1_1, c2_1, c1_2, c2_2, ...]
+  int step = 0;
+  T omega = T(0);
+  double* partials = nullptr;
+  const int* done = nullptr;  // skip when *done != 0
+  const int* gate = nullptr;  // skip when *gate == 0
+};
+
+template <typename T>
+__device__ __forceinline__ bool op_skip(const OpIO<T>& io) {
+  return (io.done && *(volatile const int*)io.done) || (io.gate && *(volatile const int*)io.gate == 0);
+}
+
+// Per-DOF epilogue; `own` is this DOF's input value (0 on fixed DOFs).
+template <typename T, int MODE>
+__device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool fx, T kv, T own, double& part) {
+  if (MODE == kModeApply) {
+    io.out[i] = fx ? io.u[i] : kv;
+  } else if (MODE == kModeResid) {
+    io.out[i] = fx ? T(0) : io.b[i] - kv;
+  } else if (MODE == kModeJacobi) {
+    io.out[i] = fx ? T(0) : own + io.omega * io.dinv[i] * (io.b[i] - kv);
+  } else if (MODE == kModeCgQ) {
+    const T q = fx ? T(0) : kv;
+    io.out[i] = q;
+    part += (double)own * (double)q;
+  } else if (MODE == kModeChebFirst) {
+    const T dd = fx ? T(0) : (T)io.coef[0] * io.dinv[i] * (io.b[i] - kv);
+    io.d[i] = dd;
+    io.out[i] = own + dd;
+  } else if (MODE == kModeChebStep) {
+    const T dd = fx ? T(0)
+                    : (T)io.coef[2 * io.step] * io.d[i] + (T)io.coef[2 * io.step + 1] * io.dinv[i] * (io.b[i] - kv);
+    io.d[i] = dd;
+    io.out[i] = own + dd;
+  } else {  // kModeDinvApply
+    io.out[i] = fx ? T(0) : io.dinv[i] * kv;
+  }
+}
 
 template <typename T, class ESrc>
 struct FineParams {
@@ -57,15 +113,9 @@ struct FineParams {
   Grid g;          // element grid
   int TY, TX, ZC;  // node tile and z chunk
   int tiles_y, tiles_x;
-  const T* u;
   const uint8_t* fix;  // per node, bit c = DOF c fixed
   ESrc esrc;
-  T* out;
-  const T* b;
-  const T* dinv;
-  T omega;
-  double* partials;
-  const int* done;  // early-exit flag (may be null)
+  OpIO<T> io;
 };
 
 // Shared memory: 3 planes x 3 comps x (TX+2)(TY+2) of T, then 2 slabs x (TX+1)(TY+1) of T.
@@ -76,7 +126,7 @@ __host__ __device__ inline size_t fine_smem_bytes(int TY, int TX) {
 
 template <typename T, int MODE, class ESrc>
 __global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__ FineParams<T, ESrc> p) {
-  if (p.done && *(volatile const int*)p.done) return;
+  if (op_skip(p.io)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);
   const int PY = p.TY + 2, PX = p.TX + 2, PP = PY * PX;
@@ -93,6 +143,7 @@ __global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__
   const int tid = threadIdx.x;
   const int ty = tid % p.TY, tx = tid / p.TY;
   const bool active = (tx < p.TX) && (x0 + tx < NX) && (y0 + ty < NY);
+  const T* __restrict__ u = p.io.u;
 
   auto stage_plane = [&](int zp) {
     const int slot = (zp + 3) % 3;
@@ -104,7 +155,7 @@ __global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__
       if (zp >= 0 && zp < NZ && gx >= 0 && gx < NX && gy >= 0 && gy < NY) {
         const long long n = p.g.nidx(gx, gy, zp);
         const int f = p.fix[n];
-        const T* un = p.u + 3 * n;
+        const T* un = u + 3 * n;
         v0 = (f & 1) ? T(0) : un[0];
         v1 = (f & 2) ? T(0) : un[1];
         v2 = (f & 4) ? T(0) : un[2];
@@ -188,30 +239,15 @@ __global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__
       }
       const long long n = p.g.nidx(x0 + tx, y0 + ty, z);
       const int f = p.fix[n];
+      const T* own = su + ((z + 3) % 3) * 3 * PP + (tx + 1) * PY + (ty + 1);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const bool fx = (f >> c) & 1;
-        const long long i = 3 * n + c;
-        if (MODE == kModeApply) {
-          p.out[i] = fx ? p.u[i] : kv[c];
-        } else if (MODE == kModeResid) {
-          p.out[i] = fx ? T(0) : p.b[i] - kv[c];
-        } else if (MODE == kModeJacobi) {
-          const T own = su[((z + 3) % 3) * 3 * PP + c * PP + (tx + 1) * PY + (ty + 1)];
-          p.out[i] = fx ? T(0) : own + p.omega * p.dinv[i] * (p.b[i] - kv[c]);
-        } else {  // kModeCgQ
-          const T own = su[((z + 3) % 3) * 3 * PP + c * PP + (tx + 1) * PY + (ty + 1)];
-          const T q = fx ? T(0) : kv[c];
-          p.out[i] = q;
-          part += (double)own * (double)q;
-        }
-      }
+      for (int c = 0; c < 3; ++c) op_epilogue<T, MODE>(p.io, 3 * n + c, (f >> c) & 1, kv[c], own[c * PP], part);
     }
     __syncthreads();
   }
   if (MODE == kModeCgQ) {
     part = block_sum(part, red);
-    if (tid == 0) p.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
+    if (tid == 0) p.io.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
   }
 }
 
@@ -254,16 +290,23 @@ __global__ void fine_diag_inv_kernel(Grid g, const __grid_constant__ KEP<double>
 __host__ __device__ constexpr int stencil_k(int jrel, int c, int d) { return (jrel * 3 + c) * 3 + d; }
 __host__ __device__ constexpr int jrel_of(int dx, int dy, int dz) { return (dz + 1) * 9 + (dx + 1) * 3 + (dy + 1); }
 
+template <typename T>
+struct StencilParams {
+  Grid g;
+  const T* A;
+  const uint8_t* fix;
+  OpIO<T> io;
+};
+
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) stencil_apply_kernel(Grid g, const T* __restrict__ A,
-                                                            const uint8_t* __restrict__ fix,
-                                                            const T* __restrict__ u, T* out, const T* b,
-                                                            const T* dinv, T omega, double* partials,
-                                                            const int* done) {
-  if (done && *(volatile const int*)done) return;
+__global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T> p) {
+  if (op_skip(p.io)) return;
   __shared__ double red[32];
+  const Grid g = p.g;
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const long long nn = g.nnode();
+  const T* __restrict__ A = p.A;
+  const T* __restrict__ u = p.io.u;
   double part = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
     const int iy = (int)(n % NY);
@@ -279,7 +322,7 @@ __global__ void __launch_bounds__(256) stencil_apply_kernel(Grid g, const T* __r
           const int x = ix + dx, y = iy + dy, z = iz + dz;
           if (x < 0 || x >= NX || y < 0 || y >= NY || z < 0 || z >= NZ) continue;
           const long long m = g.nidx(x, y, z);
-          const int fm = fix[m];
+          const int fm = p.fix[m];
           const int jr = jrel_of(dx, dy, dz);
           T um[3];
 #pragma unroll
@@ -289,27 +332,16 @@ __global__ void __launch_bounds__(256) stencil_apply_kernel(Grid g, const T* __r
 #pragma unroll
             for (int d = 0; d < 3; ++d) kv[c] = fma(__ldg(&A[(long long)stencil_k(jr, c, d) * nn + n]), um[d], kv[c]);
         }
-    const int f = fix[n];
+    const int f = p.fix[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const bool fx = (f >> c) & 1;
-      const long long i = 3 * n + c;
-      if (MODE == kModeApply) {
-        out[i] = fx ? u[i] : kv[c];
-      } else if (MODE == kModeResid) {
-        out[i] = fx ? T(0) : b[i] - kv[c];
-      } else if (MODE == kModeJacobi) {
-        out[i] = fx ? T(0) : u[i] + omega * dinv[i] * (b[i] - kv[c]);
-      } else {
-        const T q = fx ? T(0) : kv[c];
-        out[i] = q;
-        part += (double)u[i] * (double)q;
-      }
+      op_epilogue<T, MODE>(p.io, 3 * n + c, fx, kv[c], fx ? T(0) : u[3 * n + c], part);
     }
   }
   if (MODE == kModeCgQ) {
     part = block_sum(part, red);
-    if (threadIdx.x == 0) partials[blockIdx.x] = part;
+    if (threadIdx.x == 0) p.io.partials[blockIdx.x] = part;
   }
 }
 
@@ -327,13 +359,18 @@ __global__ void stencil_diag_inv_kernel(Grid g, const double* __restrict__ A, co
   }
 }
 
-// x = omega * dinv * b (first Jacobi sweep from a zero guess)
+// First smoothing step from a zero guess: x = w dinv b, with w = omega or (coef
+// given) the Chebyshev c0; d (if given) receives the same step.
 template <typename T>
-__global__ void jacobi_zero_kernel(long long ndof, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
-                                   T* x, const int* done) {
+__global__ void smooth_zero_kernel(long long ndof, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
+                                   const double* coef, T* x, T* d, const int* done) {
   if (done && *(volatile const int*)done) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x)
-    x[i] = omega * dinv[i] * b[i];
+  const T w = coef ? (T)coef[0] : omega;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x) {
+    const T v = w * dinv[i] * b[i];
+    x[i] = v;
+    if (d) d[i] = v;
+  }
 }
 
 // ----------------------------------------------------------------------------

@@ -249,49 +249,45 @@ __global__ void dense_from_stencil_kernel(Grid g, const double* __restrict__ A, 
   }
 }
 
-// In-place lower Cholesky of D (n x n, row-major), then Dinv = L^-T L^-1 into Inv.
-// One block.  *status = 0 ok, k+1 if pivot k was not positive (a shift of
-// `shift` on the diagonal is added and the factorisation retried by the host).
-__global__ void __launch_bounds__(1024) dense_inverse_kernel(int n, double* D, double* W, double* Inv, int* status) {
+// In-place Gauss-Jordan inverse of the SPD matrix D (n x n, row-major) into
+// Inv, one block, no pivoting (SPD pivots stay positive in exact arithmetic).
+// When `in_smem`, the matrix lives in dynamic shared memory (n <= 160).
+// *status = 0 ok, k+1 if pivot k was not positive.
+__global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const double* __restrict__ D, double* Inv,
+                                                                int in_smem, int* status) {
+  extern __shared__ double sA[];
+  double* A = in_smem ? sA : Inv;
   __shared__ int bad;
+  __shared__ double piv;
+  const long long nn = (long long)n * n;
+  for (long long t = threadIdx.x; t < nn; t += blockDim.x) A[t] = D[t];
   if (threadIdx.x == 0) bad = 0;
   __syncthreads();
   for (int k = 0; k < n; ++k) {
     if (threadIdx.x == 0) {
-      const double p = D[(size_t)k * n + k];
-      if (!(p > 0.0)) bad = k + 1;
-      D[(size_t)k * n + k] = sqrt(fmax(p, 1e-300));
+      const double p = A[(size_t)k * n + k];
+      if (!(p > 0.0) && !bad) bad = k + 1;
+      piv = 1.0 / (p > 0.0 ? p : 1e-300);
     }
     __syncthreads();
-    const double dkk = D[(size_t)k * n + k];
-    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) D[(size_t)i * n + k] /= dkk;
-    __syncthreads();
-    const int m = n - k - 1;
-    for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) {
-      const int i = k + 1 + (int)(t / m), j = k + 1 + (int)(t % m);
-      if (j <= i) D[(size_t)i * n + j] -= D[(size_t)i * n + k] * D[(size_t)j * n + k];
+    const double pk = piv;
+    // entries off row k and column k, from the old row/column
+    for (long long t = threadIdx.x; t < nn; t += blockDim.x) {
+      const int i = (int)(t / n), j = (int)(t % n);
+      if (i != k && j != k) A[t] -= A[(size_t)i * n + k] * A[(size_t)k * n + j] * pk;
     }
     __syncthreads();
-  }
-  // W = L^-1 (lower), column j per thread
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    for (int i = 0; i < n; ++i) {
-      double s = (i == j) ? 1.0 : 0.0;
-      if (i < j) {
-        W[(size_t)i * n + j] = 0.0;
-        continue;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      if (t != k) {
+        A[(size_t)t * n + k] *= -pk;  // column k
+        A[(size_t)k * n + t] *= pk;   // row k
       }
-      for (int k = j; k < i; ++k) s -= D[(size_t)i * n + k] * W[(size_t)k * n + j];
-      W[(size_t)i * n + j] = s / D[(size_t)i * n + i];
     }
+    if (threadIdx.x == 0) A[(size_t)k * n + k] = pk;
+    __syncthreads();
   }
-  __syncthreads();
-  for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
-    const int i = (int)(t / n), j = (int)(t % n);
-    double s = 0.0;
-    for (int k = max(i, j); k < n; ++k) s += W[(size_t)k * n + i] * W[(size_t)k * n + j];
-    Inv[t] = s;
-  }
+  if (in_smem)
+    for (long long t = threadIdx.x; t < nn; t += blockDim.x) Inv[t] = A[t];
   if (threadIdx.x == 0) *status = bad;
 }
 

@@ -33,6 +33,7 @@ from .stiffness import lk_H8
 logger = logging.getLogger(__name__)
 
 EMIN = 1.0e-9
+EVAL_RTOL = 1.0e-12  # fixed-geometry evaluations (optimizer.py:54-279 solve directly)
 
 
 def _fixed_dof_mask(nelx, nely, nelz, support_mask):
@@ -398,9 +399,14 @@ def top3d(
     final_rho_filtered = from_flat(S.rho_f, expected_shape).cpu().numpy()
     final_xPhys = from_flat(S.rho_p, expected_shape).cpu().numpy()
 
+    solver.close()
+    # Final and binary designs are evaluated by a tight FP64 solve: thresholded
+    # designs with 1e-9 voids are far worse conditioned than the loop's iterates.
+    eval_solver = HexSolver(nelx, nely, nelz, KE, _fixed_dof_mask(nelx, nely, nelz, support_mask),
+                            precision="fp64", rtol=EVAL_RTOL, max_iterations=20000)
     ev = dict(penal=penal, material_params=material_params, elem_size=elem_size, force_field=force_field,
               support_mask=support_mask, obstacle_mask=obstacle_mask,
-              protected_zone_mask=protected_zone_mask, _solver=solver, _F=Fd)
+              protected_zone_mask=protected_zone_mask, _solver=eval_solver, _F=Fd)
     final_compliance = evaluate_fixed_geometry_compliance(xPhys=final_xPhys, **ev)
     if save_history:
         history["density_history"].append(final_xPhys.copy())
@@ -442,7 +448,7 @@ def top3d(
     if diagnostics_out is not None:
         diagnostics_out.clear()
         diagnostics_out.update(metrics)
-    solver.close()
+    eval_solver.close()
     return final_xPhys, history, final_compliance, None
 
 
@@ -470,7 +476,7 @@ def evaluate_fixed_geometry_metrics(xPhys, penal, material_params=None, elem_siz
     solver = _solver
     if solver is None:
         solver = HexSolver(nelx, nely, nelz, KE, _fixed_dof_mask(nelx, nely, nelz, support_mask),
-                           precision=precision)
+                           precision=precision, rtol=EVAL_RTOL, max_iterations=20000)
     rho = to_flat(x_eval)
     solver.set_density(rho, penal)
     E = EMIN + (1.0 - EMIN) * rho ** penal

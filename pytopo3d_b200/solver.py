@@ -6,9 +6,12 @@ Replaces the reference's solve boundary: the per-iteration CSR assembly and
 
 * ``precision="fp64"``: FP64 operator, FP64 multigrid V-cycle, PCG to the
   relative residual ``rtol`` (default 1e-10);
-* ``precision="mixed"``: FP32 operator with BF16 densities, FP32 smoother and
-  CG vectors (FP64 dot products) inside FP64 iterative refinement whose
-  residual ``f - K u`` and update of ``u`` are FP64.
+* ``precision="mixed"``: CG whose operator, multigrid V-cycle and vectors are
+  FP32 (fine operator from FP32 moduli, or BF16 densities with
+  ``inner_density=1``), FP64 dot products, and FP64 reliable updates: the FP32
+  iterate is folded into the FP64 solution and the FP64 residual ``f - K u``
+  replaces the FP32 one whenever the latter has fallen by ``reliable_delta``;
+  convergence is decided on the FP64 residual.
 
 Non-convergence raises ``RuntimeError`` like the reference's CuPy path
 (solver.py:57-58).
@@ -24,9 +27,6 @@ import torch
 
 from . import _lib
 from ._tensors import device, vec
-
-DEFAULTS = dict(max_iterations=2000, rtol=1e-10, pre_sweeps=2, post_sweeps=2, omega=0.6,
-                coarsest_max_dofs=500, max_levels=12, inner_rtol=1e-4, max_refinements=30)
 
 
 class HexSolver:
@@ -107,8 +107,8 @@ class HexSolver:
     def stats(self) -> dict:
         buf = (C.c_double * 16)()
         n = _lib.lib().tp3d_solver_stats(self._h, buf, 16)
-        keys = ["levels", "iterations", "refinements", "relres", "inner_iterations", "coarsest_dofs",
-                "tile_y", "tile_x", "z_chunk"]
+        keys = ["levels", "iterations", "reliable_updates", "relres", "restarts", "coarsest_dofs",
+                "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
 
 

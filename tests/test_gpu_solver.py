@@ -57,12 +57,20 @@ def test_apply_matches_assembled_matrix(P, dims):
         y = s.apply(torch.as_tensor(u).cuda()).cpu().numpy()
         np.testing.assert_allclose(y, y_ref, rtol=0, atol=1e-13 * np.abs(y_ref).max())
         if prec == "mixed":
-            # BF16 densities: compare with the operator of the rounded densities
-            rho16 = torch.as_tensor(rho).to(torch.bfloat16).double().numpy()
-            y16_ref = _oracle_apply(rho16, KE, 3.0, nx, ny, nz, fmask, u.astype(np.float32).astype(float))
+            # FP32 operator (FP32 moduli) against the FP64 assembled operator
+            u32 = u.astype(np.float32).astype(float)
+            y32_ref = _oracle_apply(rho, KE, 3.0, nx, ny, nz, fmask, u32)
             y32 = s.apply(torch.as_tensor(u, dtype=torch.float32).cuda()).double().cpu().numpy()
-            np.testing.assert_allclose(y32, y16_ref, rtol=0, atol=2e-6 * np.abs(y16_ref).max())
+            np.testing.assert_allclose(y32, y32_ref, rtol=0, atol=2e-6 * np.abs(y32_ref).max())
         s.close()
+    # BF16-density FP32 operator against the operator of the rounded densities
+    s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", inner_density=1)
+    s.set_density(to_flat(rho), 3.0)
+    rho16 = torch.as_tensor(rho).to(torch.bfloat16).double().numpy()
+    y16_ref = _oracle_apply(rho16, KE, 3.0, nx, ny, nz, fmask, u.astype(np.float32).astype(float))
+    y16 = s.apply(torch.as_tensor(u, dtype=torch.float32).cuda()).double().cpu().numpy()
+    np.testing.assert_allclose(y16, y16_ref, rtol=0, atol=2e-6 * np.abs(y16_ref).max())
+    s.close()
 
 
 @pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
@@ -85,8 +93,9 @@ def test_fp64_solve_matches_reference_direct_solve(P, golden, tag):
     s.close()
 
 
-@pytest.mark.parametrize("dims", [(16, 8, 8), (24, 12, 12), (20, 7, 9)])
-def test_mixed_precision_matches_fp64(P, dims):
+@pytest.mark.parametrize("dims,opts", [((16, 8, 8), {}), ((24, 12, 12), {}), ((20, 7, 9), {}),
+                                       ((24, 12, 12), {"inner_density": 1})])
+def test_mixed_precision_matches_fp64(P, dims, opts):
     from pytopo3d_b200._tensors import to_flat
     from pytopo3d_b200.solver import HexSolver
 
@@ -98,16 +107,36 @@ def test_mixed_precision_matches_fp64(P, dims):
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, ndof)).cuda()
     out = {}
     for prec in ("fp64", "mixed"):
-        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec)
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, **opts)
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
-        assert s.last_relres <= 1e-10
+        # 1e-9 void pockets put an attainable floor on the true residual; the
+        # solver accepts it only once restarts / reliable updates stop gaining
+        assert s.last_relres <= 1e-10 or (s.stats()["residual_floor"] and s.last_relres <= 1e-7)
         out[prec] = U.cpu().numpy()
         s.close()
     Fh = F.cpu().numpy()
     c64, c32 = Fh @ out["fp64"], Fh @ out["mixed"]
     assert abs(c32 - c64) <= 1e-6 * abs(c64)
     assert np.linalg.norm(out["mixed"] - out["fp64"]) <= 1e-6 * np.linalg.norm(out["fp64"])
+
+
+def test_damped_jacobi_smoother_option(P):
+    # damped Jacobi (omega 0.6) is stable for grey designs without voids
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 16, 8, 8
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=3, lo=0.2)
+    F = O.build_force_vector(nx, ny, nz, fmask.size)
+    Uref, _ = O.solve_displacement(rho, KE, 3.0, F, free, nx, ny, nz)
+    for prec in ("fp64", "mixed"):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, smoother=1)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(torch.as_tensor(F).cuda()).cpu().numpy()
+        np.testing.assert_allclose(U, Uref, rtol=0, atol=1e-7 * np.abs(Uref).max())
+        s.close()
 
 
 def test_multigrid_and_jacobi_agree_with_spsolve(P):
