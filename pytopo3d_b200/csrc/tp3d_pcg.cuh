@@ -20,7 +20,8 @@ struct PcgState {
   int update;   // mixed precision: replace the residual this iteration
   int updates;  // count of reliable updates
   int stall;    // consecutive reliable updates that did not halve the FP64 residual
-  int pad[2];
+  int restart;  // mixed precision: FP32 p'Ap <= 0, restart the direction from z
+  int nbreak;   // consecutive restarts
 };
 
 enum FinalizeOp : int {
@@ -33,12 +34,14 @@ enum FinalizeOp : int {
   kFinRRMixed,   // FP32 recursive residual: decide on a reliable update
   kFinRRHi,      // FP64 true residual after a reliable update: stop test
   kFinValue,     // plain sum into *out (no state change)
+  kFinPQMixed,   // as kFinPQ, but a non-positive FP32 p'Ap restarts the direction
+  kFinRZMixed,   // as kFinRZ, honouring a pending restart (beta = 0)
 };
 
 __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgState* st, int op, double rtol2,
                                 double* out) {
   __shared__ double red[32];
-  if ((op >= kFinPQ && op <= kFinRRMixed) && *(volatile int*)&st->done) return;
+  if (((op >= kFinPQ && op <= kFinRRMixed) || op >= kFinPQMixed) && *(volatile int*)&st->done) return;
   if (op == kFinRRHi && (*(volatile int*)&st->done || *(volatile int*)&st->update == 0)) return;
   const double s = sum_partials(partials, n, red);
   if (threadIdx.x != 0) return;
@@ -86,7 +89,9 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
       if (!isfinite(s)) {
         st->done = 4;
       } else {
-        st->update = (s <= st->delta2 * st->rmax2 || s <= st->tol2 || st->iters >= st->max_iters) ? 1 : 0;
+        st->update = (st->restart || s <= st->delta2 * st->rmax2 || s <= st->tol2 || st->iters >= st->max_iters)
+                         ? 1
+                         : 0;
       }
       break;
     case kFinRRHi:
@@ -106,6 +111,31 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
       break;
     case kFinValue:
       *out = s;
+      break;
+    case kFinPQMixed:
+      // FP32 rounding next to 1e-9 voids can make p'Ap non-positive although K
+      // is SPD: skip the step (alpha = 0), force a reliable update and restart
+      // the direction from the new preconditioned residual.
+      st->pq = s;
+      if (!isfinite(s)) {
+        st->done = 4;
+      } else if (!(s > 0.0)) {
+        st->alpha = 0.0;
+        st->restart = 1;
+        if (++st->nbreak > 5) st->done = 3;
+      } else {
+        st->alpha = st->rz / s;
+      }
+      break;
+    case kFinRZMixed:
+      if (st->restart) {
+        st->beta = 0.0;
+        st->restart = 0;
+      } else {
+        st->beta = s / st->rz;
+        st->nbreak = 0;
+      }
+      st->rz = s;
       break;
   }
 }

@@ -511,7 +511,8 @@ struct tp3d_solver {
     io.partials = partials;
     io.done = done;
     int rc = fine<float, kModeCgQ>(io);
-    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials(), state, kFinPQ, 0.0, nullptr); count_launch();
+    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials(), state, kFinPQMixed, 0.0, nullptr);
+    count_launch();
     cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials); count_launch();
     finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRMixed, 0.0, nullptr); count_launch();
     // reliable update (every kernel below is a no-op unless state->update)
@@ -531,7 +532,7 @@ struct tp3d_solver {
     clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
     float* z = vcycle<float>(0, K.r, done, &rc);
     dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZ, 0.0, nullptr); count_launch();
+    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZMixed, 0.0, nullptr); count_launch();
     cg_p_kernel<float><<<nb, 256, 0, st>>>(ndof, z, K.p, state, 0); count_launch();
     TP3D_CHECK_LAUNCH();
     return rc;
