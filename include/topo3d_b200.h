@@ -112,6 +112,26 @@ int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const double* x,
                    double bisection_tol, double* x_new, double* rho_new, double* stats,
                    void* scratch, void* stream);
 
+/* The same OC update without any device allocation, for callers that must
+ * not allocate device memory per call (an application whose device memory
+ * is reserved up front by its own allocator, or code that cannot accept the
+ * implicit device synchronisation of cudaMalloc / cudaFree).  No counterpart
+ * in the reference: it is an addition of this library.
+ * Scratch is one file-scope __device__ array (about 2.2 MB) that every GPU
+ * loading this library holds until exit; grids above
+ * tp3d_oc_noalloc_max_elements() (262144) elements are rejected with
+ * TP3D_ERR_ARG.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU race; issue them
+ * on one stream.  Arguments and results are those of tp3d_oc_update. */
+long long tp3d_oc_noalloc_max_elements(void);
+int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin, const double* x,
+                           const double* dc_dx, const double* dv_dx, const double* Hs,
+                           const uint8_t* solid, const uint8_t* void_, double move,
+                           double target_free_volume, double beta, double eta, int max_bisection,
+                           double bisection_tol, double* x_new, double* rho_new, double* stats,
+                           void* stream);
+
 /* ---------------------------------------------------------------------------
  * Matrix-free H8 elasticity solver (multigrid-preconditioned CG)
  * ------------------------------------------------------------------------- */

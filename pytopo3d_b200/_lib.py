@@ -65,6 +65,9 @@ SIGNATURES = {
     "tp3d_oc_scratch_bytes": (sz, [i32, i32, i32, f64]),
     "tp3d_oc_update": (i32, [i32, i32, i32, f64, vp, vp, vp, vp, vp, vp, f64, f64, f64, f64, i32, f64, vp, vp,
                              vp, vp, vp]),
+    "tp3d_oc_noalloc_max_elements": (i64, []),
+    "tp3d_oc_update_noalloc": (i32, [i32, i32, i32, f64, vp, vp, vp, vp, vp, vp, f64, f64, f64, f64, i32, f64, vp,
+                                     vp, vp, vp]),
     "tp3d_solver_default_opts": (None, [C.POINTER(SolverOpts)]),
     "tp3d_solver_create": (i32, [i32, i32, i32, vp, vp, C.POINTER(SolverOpts), vp, C.POINTER(vp)]),
     "tp3d_solver_destroy": (i32, [vp]),

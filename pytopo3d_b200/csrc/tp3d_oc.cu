@@ -12,6 +12,8 @@
 // recomputed from it at the end, so no candidate array is stored.
 #include <cfloat>
 #include <cmath>
+#include <mutex>
+#include <vector>
 
 #include "tp3d_filter.cuh"
 
@@ -227,6 +229,178 @@ extern "C" int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const d
   const size_t smem = (size_t)filter_smem_elems(fc.Z) * sizeof(double);
   const long long ntiles = filter_ntiles(g);
   TP3D_DISPATCH_Z(fc.Z, {
+    auto kern = oc_kernel<ZC>;
+    TP3D_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TP3D_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFilterThreads, smem));
+    if (per_sm < 1) {
+      tp3d_set_last_error("OC kernel does not fit on an SM");
+      return TP3D_ERR_CUDA;
+    }
+    long long grid = std::min<long long>((long long)per_sm * nsm, ntiles);
+    grid = std::min<long long>(grid, kOcMaxBlocks);
+    void* args[] = {&a};
+    TP3D_CHECK(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)grid), dim3(kFilterThreads), args,
+                                           smem, st));
+  });
+  add_launches(1);
+  return TP3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// OC update without device allocation.
+//
+// For callers that must not allocate device memory per call: an application
+// whose device memory is fully reserved up front by its own allocator, or code
+// that cannot accept the implicit device synchronisation that cudaMalloc /
+// cudaFree bring.  The scratch of the bisection (normalised ratios, per-block
+// partial sums, barrier counters, filter column table) lives in one
+// file-scope __device__ array instead.  Every GPU that loads this library
+// holds that array (about 2.2 MB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long long kNoAllocMaxElements = 1LL << 18;  // e.g. 64x64x64 or 128x64x32
+constexpr int kNoAllocMaxCols = (2 * kFilterMaxZ + 1) * (2 * kFilterMaxZ + 1);
+constexpr size_t kNoAllocRatioBytes = (size_t)kNoAllocMaxElements * sizeof(double);
+constexpr size_t kNoAllocPartBytes = (size_t)3 * kOcMaxBlocks * sizeof(double);
+constexpr size_t kNoAllocBarrierBytes = 256;
+constexpr size_t kNoAllocDxyBytes = ((kNoAllocMaxCols * sizeof(int2) + 255) / 256) * 256;
+constexpr size_t kNoAllocWBytes = (size_t)kNoAllocMaxCols * (2 * kFilterMaxZ + 1) * sizeof(double);
+constexpr size_t kNoAllocBytes =
+    kNoAllocRatioBytes + kNoAllocPartBytes + kNoAllocBarrierBytes + kNoAllocDxyBytes + kNoAllocWBytes;
+
+static __device__ __align__(256) unsigned char g_oc_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};  // per device: device address of g_oc_noalloc_scratch
+
+// Device address of the static scratch on the current device; looked up once per
+// device with that device current.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  TP3D_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    tp3d_set_last_error("device ordinal out of range for the static OC scratch");
+    return TP3D_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_oc_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      tp3d_set_last_error(e != cudaSuccess ? cudaGetErrorString(e) : "null symbol address");
+      return TP3D_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return TP3D_OK;
+}
+
+// Filter columns for rmin, built on the host in the same order as the
+// allocating path's table (rmin - |d| > 1e-9, grouped by (dx, dy)).
+int noalloc_columns(double rmin, int* Z, std::vector<int2>* dxy, std::vector<double>* w) {
+  if (!(rmin > 0.0) || !std::isfinite(rmin)) return TP3D_ERR_ARG;
+  const int R = (int)std::ceil(rmin) + 1;
+  int z = 0;
+  for (int d = 0; d <= R; ++d)
+    if (rmin - std::sqrt((double)(d * d)) > 1e-9) z = d;
+  if (z > kFilterMaxZ) {
+    tp3d_set_last_error("rmin too large for the stencil filter (max 7)");
+    return TP3D_ERR_ARG;
+  }
+  const int W = 2 * z + 1;
+  for (int dx = -z; dx <= z; ++dx)
+    for (int dy = -z; dy <= z; ++dy) {
+      std::vector<double> col(W, 0.0);
+      bool any = false;
+      for (int dz = -z; dz <= z; ++dz) {
+        const double wt = rmin - std::sqrt((double)(dx * dx + dy * dy + dz * dz));
+        if (wt > 1e-9) {
+          col[dz + z] = wt;
+          any = true;
+        }
+      }
+      if (any) {
+        dxy->push_back(make_int2(dx, dy));
+        w->insert(w->end(), col.begin(), col.end());
+      }
+    }
+  *Z = z;
+  return TP3D_OK;
+}
+
+}  // namespace
+
+extern "C" long long tp3d_oc_noalloc_max_elements(void) { return kNoAllocMaxElements; }
+
+extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin, const double* x,
+                                      const double* dc_dx, const double* dv_dx, const double* Hs,
+                                      const uint8_t* solid, const uint8_t* void_, double move,
+                                      double target_free_volume, double beta, double eta, int max_bisection,
+                                      double bisection_tol, double* x_new, double* rho_new, double* stats,
+                                      void* stream) {
+  if (nelx < 1 || nely < 1 || nelz < 1 || !x || !dc_dx || !dv_dx || !Hs || !x_new || !rho_new || !stats)
+    return TP3D_ERR_ARG;
+  const long long n = (long long)nelx * nely * nelz;
+  if (n > kNoAllocMaxElements) {
+    tp3d_set_last_error(
+        "tp3d_oc_update_noalloc: the grid has more elements than the static scratch holds (max 262144); "
+        "use tp3d_oc_update with caller-provided scratch");
+    return TP3D_ERR_ARG;
+  }
+  if (!std::isfinite(move) || move <= 0.0) {
+    tp3d_set_last_error("move must be positive");
+    return TP3D_ERR_ARG;
+  }
+  if (max_bisection < 1) {
+    tp3d_set_last_error("max_bisection_iterations must be at least 1");
+    return TP3D_ERR_ARG;
+  }
+  if (!std::isfinite(beta) || beta <= 0.0 || !(eta > 0.0 && eta < 1.0)) {
+    tp3d_set_last_error("invalid projection parameters");
+    return TP3D_ERR_ARG;
+  }
+  int Z = 0;
+  std::vector<int2> dxy;
+  std::vector<double> w;
+  if (int rc = noalloc_columns(rmin, &Z, &dxy, &w)) return rc;
+  void* base_v = nullptr;
+  if (int rc = noalloc_scratch(&base_v)) return rc;
+  unsigned char* base = (unsigned char*)base_v;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  const Grid g{nelx, nely, nelz};
+  OcArgs a{g, FilterCols{}, x, dc_dx, dv_dx, Hs, solid, void_, move, target_free_volume, bisection_tol,
+           max_bisection, Projection(beta, eta), x_new, rho_new, stats};
+  a.ratio = (double*)base;
+  a.partA = (double*)(base + kNoAllocRatioBytes);
+  a.partB = a.partA + kOcMaxBlocks;
+  a.partC = a.partB + kOcMaxBlocks;
+  unsigned int* bar = (unsigned int*)(base + kNoAllocRatioBytes + kNoAllocPartBytes);
+  a.bar.count = bar;
+  a.bar.gen = bar + 1;
+  a.bar.err = (int*)(bar + 2);
+  int2* d_dxy = (int2*)(base + kNoAllocRatioBytes + kNoAllocPartBytes + kNoAllocBarrierBytes);
+  double* d_w = (double*)((unsigned char*)d_dxy + kNoAllocDxyBytes);
+  a.fc.dxy = d_dxy;
+  a.fc.w = d_w;
+  a.fc.ncols = (int)dxy.size();
+  a.fc.Z = Z;
+  // The array keeps the previous call's contents: the column table is
+  // rewritten and the barrier counters cleared on every call.
+  TP3D_CHECK(cudaMemcpyAsync(d_dxy, dxy.data(), dxy.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+  TP3D_CHECK(cudaMemcpyAsync(d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  TP3D_CHECK(cudaMemsetAsync(bar, 0, kNoAllocBarrierBytes, st));
+  TP3D_CHECK(cudaMemsetAsync(stats, 0xff, 8 * sizeof(double), st));
+
+  int dev = 0, nsm = 0;
+  TP3D_CHECK(cudaGetDevice(&dev));
+  TP3D_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const size_t smem = (size_t)filter_smem_elems(Z) * sizeof(double);
+  const long long ntiles = filter_ntiles(g);
+  TP3D_DISPATCH_Z(Z, {
     auto kern = oc_kernel<ZC>;
     TP3D_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
