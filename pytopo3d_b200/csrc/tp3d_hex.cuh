@@ -107,149 +107,6 @@ __device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool
   }
 }
 
-template <typename T, class ESrc>
-struct FineParams {
-  KEP<T> ke;
-  Grid g;          // element grid
-  int TY, TX, ZC;  // node tile and z chunk
-  int tiles_y, tiles_x;
-  const uint8_t* fix;  // per node, bit c = DOF c fixed
-  ESrc esrc;
-  OpIO<T> io;
-};
-
-// Shared memory: 3 planes x 3 comps x (TX+2)(TY+2) of T, then 2 slabs x (TX+1)(TY+1) of T.
-template <typename T>
-__host__ __device__ inline size_t fine_smem_bytes(int TY, int TX) {
-  return (size_t)(9 * (TX + 2) * (TY + 2) + 2 * (TX + 1) * (TY + 1)) * sizeof(T);
-}
-
-template <typename T, int MODE, class ESrc>
-__global__ void __launch_bounds__(256) fine_apply_kernel(const __grid_constant__ FineParams<T, ESrc> p) {
-  if (op_skip(p.io)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* su = reinterpret_cast<T*>(smem_raw);
-  const int PY = p.TY + 2, PX = p.TX + 2, PP = PY * PX;
-  T* se = su + 9 * PP;
-  const int EY = p.TY + 1, EX = p.TX + 1, EP = EY * EX;
-  __shared__ double red[32];
-
-  const int NX = p.g.nx + 1, NY = p.g.ny + 1, NZ = p.g.nz + 1;
-  const int by = blockIdx.x % p.tiles_y;
-  const int bx = blockIdx.x / p.tiles_y;
-  const int x0 = bx * p.TX, y0 = by * p.TY;
-  const int zb = blockIdx.y * p.ZC;
-  const int ze = min(zb + p.ZC, NZ);
-  const int tid = threadIdx.x;
-  const int ty = tid % p.TY, tx = tid / p.TY;
-  const bool active = (tx < p.TX) && (x0 + tx < NX) && (y0 + ty < NY);
-  const T* __restrict__ u = p.io.u;
-
-  auto stage_plane = [&](int zp) {
-    const int slot = (zp + 3) % 3;
-    T* dst = su + slot * 3 * PP;
-    for (int i = tid; i < PP; i += blockDim.x) {
-      const int ly = i % PY, lx = i / PY;
-      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-      T v0 = T(0), v1 = T(0), v2 = T(0);
-      if (zp >= 0 && zp < NZ && gx >= 0 && gx < NX && gy >= 0 && gy < NY) {
-        const long long n = p.g.nidx(gx, gy, zp);
-        const int f = p.fix[n];
-        const T* un = u + 3 * n;
-        v0 = (f & 1) ? T(0) : un[0];
-        v1 = (f & 2) ? T(0) : un[1];
-        v2 = (f & 4) ? T(0) : un[2];
-      }
-      dst[i] = v0;
-      dst[PP + i] = v1;
-      dst[2 * PP + i] = v2;
-    }
-  };
-  auto stage_slab = [&](int zs) {
-    T* dst = se + ((zs + 2) % 2) * EP;
-    for (int i = tid; i < EP; i += blockDim.x) {
-      const int ly = i % EY, lx = i / EY;
-      const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-      T v = T(0);
-      if (zs >= 0 && zs < p.g.nz && gx >= 0 && gx < p.g.nx && gy >= 0 && gy < p.g.ny)
-        v = (T)p.esrc(p.g.eidx(gx, gy, zs));
-      dst[i] = v;
-    }
-  };
-
-  double part = 0.0;
-  stage_plane(zb - 1);
-  stage_plane(zb);
-  stage_slab(zb - 1);
-  for (int z = zb; z < ze; ++z) {
-    stage_plane(z + 1);
-    stage_slab(z);
-    __syncthreads();
-    if (active) {
-      T acc[8][3];
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) acc[e][c] = T(0);
-#pragma unroll
-      for (int dz = -1; dz <= 1; ++dz) {
-        const T* pl = su + ((z + dz + 3) % 3) * 3 * PP;
-#pragma unroll
-        for (int dx = -1; dx <= 1; ++dx) {
-#pragma unroll
-          for (int dy = -1; dy <= 1; ++dy) {
-            const int off = (tx + 1 + dx) * PY + (ty + 1 + dy);
-            const T um0 = pl[off], um1 = pl[PP + off], um2 = pl[2 * PP + off];
-#pragma unroll
-            for (int ez = -1; ez <= 0; ++ez)
-#pragma unroll
-              for (int ex = -1; ex <= 0; ++ex)
-#pragma unroll
-                for (int ey = -1; ey <= 0; ++ey) {
-                  const int ox = dx - ex, oy = dy - ey, oz = dz - ez;
-                  if (ox < 0 || ox > 1 || oy < 0 || oy > 1 || oz < 0 || oz > 1) continue;
-                  const int a = corner_index(-ex, -ey, -ez);
-                  const int b = corner_index(ox, oy, oz);
-                  const int e8 = (ez + 1) * 4 + (ey + 1) * 2 + (ex + 1);
-#pragma unroll
-                  for (int c = 0; c < 3; ++c) {
-                    T t = acc[e8][c];
-                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 0], um0, t);
-                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 1], um1, t);
-                    t = fma(p.ke.k[(3 * a + c) * 24 + 3 * b + 2], um2, t);
-                    acc[e8][c] = t;
-                  }
-                }
-          }
-        }
-      }
-      T kv[3] = {T(0), T(0), T(0)};
-#pragma unroll
-      for (int ez = -1; ez <= 0; ++ez) {
-        const T* sl = se + ((z + ez + 2) % 2) * EP;
-#pragma unroll
-        for (int ex = -1; ex <= 0; ++ex)
-#pragma unroll
-          for (int ey = -1; ey <= 0; ++ey) {
-            const T E = sl[(tx + 1 + ex) * EY + (ty + 1 + ey)];
-            const int e8 = (ez + 1) * 4 + (ey + 1) * 2 + (ex + 1);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) kv[c] = fma(E, acc[e8][c], kv[c]);
-          }
-      }
-      const long long n = p.g.nidx(x0 + tx, y0 + ty, z);
-      const int f = p.fix[n];
-      const T* own = su + ((z + 3) % 3) * 3 * PP + (tx + 1) * PY + (ty + 1);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) op_epilogue<T, MODE>(p.io, 3 * n + c, (f >> c) & 1, kv[c], own[c * PP], part);
-    }
-    __syncthreads();
-  }
-  if (MODE == kModeCgQ) {
-    part = block_sum(part, red);
-    if (tid == 0) p.io.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
-  }
-}
 
 // Diagonal of the fine operator: D[n,c] = sum_e E_e KE[3a+c][3a+c]; 1 on fixed DOFs.
 // Writes its inverse.

@@ -14,7 +14,8 @@ struct PcgState {
   double rr_hi;    // last FP64 residual norm^2
   double rr_best;  // smallest FP64 residual norm^2 so far
   // done: 0 running, 1 converged, 2 iteration cap, 3 breakdown, 4 non-finite,
-  //       5 FP64 residual stalled at its attainable floor (accepted)
+  //       5 FP64 residual stalled at its attainable floor (accepted),
+  //       6 FP64 residual stalled far above the target (mixed: fall back to FP64)
   int done;
   int iters, max_iters;
   int update;   // mixed precision: replace the residual this iteration
@@ -105,7 +106,9 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
       } else {
         st->stall = (s > 0.25 * st->rr_best) ? st->stall + 1 : 0;
         st->rr_best = fmin(st->rr_best, s);
-        if (st->stall >= 3) st->done = 5;
+        // a stall is an attainable floor only once the residual is small; a stall
+        // above 1e-6 relative is a failure (the host then falls back to FP64)
+        if (st->stall >= 3) st->done = (s <= 1e-12 * st->bb) ? 5 : 6;
         else if (st->iters >= st->max_iters) st->done = 2;
       }
       break;

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 
+#include "tp3d_fine.cuh"
 #include "tp3d_pcg.cuh"
 
 namespace tp3d {
@@ -56,26 +57,88 @@ struct KrylovVec {
 };
 
 struct Tile {
-  int TY = 32, TX = 8, ZC = 8, tiles_y = 1, tiles_x = 1, zchunks = 1, threads = 256;
+  int TY = 32, TX = 8, ZC = 8, tiles_y = 1, tiles_x = 1, zchunks = 1, threads = 256, occ = 0;
 };
 
-// Node-plane tile (TY x TX <= 256 threads) with little padding waste, and a
-// z chunk that still gives every SM a few blocks.
+// Launch / occupancy of the fine operator for a compile-time tile height.
+template <typename T, class ESrc, bool CLS>
+int fine_launch_t(const FineParams<T, ESrc>& p, int TY, dim3 grid, int threads, cudaStream_t st) {
+  constexpr int NZT = sizeof(T) == 4 ? 2 : 1;
+  switch (TY) {
+#define TP3D_FINE_CASE(ty)                                                                             \
+  case ty:                                                                                             \
+    fine_apply_kernel<T, ESrc, ty, NZT, CLS><<<grid, threads, fine_smem_bytes<T, ty, NZT>(), st>>>(p); \
+    return TP3D_OK;
+    TP3D_FINE_TY_LIST(TP3D_FINE_CASE)
+#undef TP3D_FINE_CASE
+  }
+  return TP3D_ERR_ARG;
+}
+template <typename T, class ESrc>
+int fine_launch(const FineParams<T, ESrc>& p, int TY, bool cls, dim3 grid, int threads, cudaStream_t st) {
+  return cls ? fine_launch_t<T, ESrc, true>(p, TY, grid, threads, st)
+             : fine_launch_t<T, ESrc, false>(p, TY, grid, threads, st);
+}
+
+template <typename T, class ESrc>
+int fine_occupancy(int TY, int threads) {
+  constexpr int NZT = sizeof(T) == 4 ? 2 : 1;
+  int occ = 0;
+  switch (TY) {
+#define TP3D_FINE_CASE(ty)                                                                                      \
+  case ty:                                                                                                      \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fine_apply_kernel<T, ESrc, ty, NZT, true>, threads,     \
+                                                  fine_smem_bytes<T, ty, NZT>());                               \
+    break;
+    TP3D_FINE_TY_LIST(TP3D_FINE_CASE)
+#undef TP3D_FINE_CASE
+  }
+  return std::max(occ, 1);
+}
+
+// Class values of KE when it has the cubic-symmetry structure of kKEClassHost
+// (entry = sign * class value, checked to 1e-12 of max |KE|); false otherwise.
+bool ke_classes(const double* KE, double* vals) {
+  double mx = 0.0;
+  for (int i = 0; i < 576; ++i) mx = std::max(mx, std::fabs(KE[i]));
+  bool have[kKEClasses] = {};
+  for (int i = 0; i < 576; ++i) {
+    const int t = kKEClassHost[i];
+    if (t == 0) continue;
+    const int k = std::abs(t) - 1;
+    if (!have[k]) {
+      vals[k] = t > 0 ? KE[i] : -KE[i];
+      have[k] = true;
+    }
+  }
+  for (int i = 0; i < 576; ++i) {
+    const int t = kKEClassHost[i];
+    const double rec = t == 0 ? 0.0 : (t > 0 ? vals[std::abs(t) - 1] : -vals[std::abs(t) - 1]);
+    if (std::fabs(rec - KE[i]) > 1e-12 * mx) return false;
+  }
+  return true;
+}
+
+// Node-plane tile from the compile-time heights (TY) and a run-time width
+// (TX, TY*TX <= 256) with little padding and halo waste; then the z chunk
+// (a multiple of the nodes per step) that fills the resident block slots in
+// whole waves at the lowest prologue cost.
+template <typename T, class ESrc>
 Tile choose_tile(const Grid& g, int nsm) {
+  constexpr int NZT = sizeof(T) == 4 ? 2 : 1;
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  static const int kMenu[] = {8, 13, 16, 17, 24, 32, 33, 43, 64};
   Tile best;
   double best_cost = 1e300;
-  for (int ky = 1; ky <= NY; ++ky) {
-    const int TY = (NY + ky - 1) / ky;
-    if (TY > 64) continue;
-    if (TY < 8 && ky > 1) break;
-    for (int kx = 1; kx <= NX; ++kx) {
-      const int TX = (NX + kx - 1) / kx;
-      if (TY * TX > 256) continue;
+  for (int TY : kMenu) {
+    const int ky = (NY + TY - 1) / TY;
+    for (int TX = 1; TX * TY <= 256; ++TX) {
       const int thr = ((TY * TX + 31) / 32) * 32;
+      if ((TY + 2) * (TX + 2) > 2 * thr || (TY + 1) * (TX + 1) > 2 * thr) continue;
+      const int kx = (NX + TX - 1) / TX;
       const double slots = (double)ky * kx * thr;
       const double halo = (double)(TY + 2) * (TX + 2) / ((double)TY * TX);
-      const double cost = slots * (1.0 + 0.35 * (halo - 1.0)) * (thr < 128 ? 1.3 : 1.0);
+      const double cost = slots * (1.0 + 0.3 * (halo - 1.0)) * (thr < 96 ? 1.5 : 1.0);
       if (cost < best_cost) {
         best_cost = cost;
         best.TY = TY;
@@ -84,14 +147,26 @@ Tile choose_tile(const Grid& g, int nsm) {
         best.tiles_x = kx;
         best.threads = thr;
       }
-      break;
     }
   }
+  best.occ = fine_occupancy<T, ESrc>(best.TY, best.threads);
   const long long planes = (long long)best.tiles_y * best.tiles_x;
-  int zc = 32;
-  while (zc > 8 && planes * ((NZ + zc - 1) / zc) < 2LL * nsm) zc /= 2;
-  best.ZC = zc;
-  best.zchunks = (NZ + zc - 1) / zc;
+  // Relative throughput of an SM running L co-resident blocks (latency hiding).
+  auto eff = [&](long long L) {
+    const long long l = std::min<long long>(L, best.occ);
+    return l <= 1 ? 1.0 : (l == 2 ? 1.5 : (l == 3 ? 1.75 : 1.9));
+  };
+  double best_t = 1e300;
+  for (int zc = NZT; zc <= std::max(NZT, NZ + NZT); zc += NZT) {
+    const long long nch = (NZ + zc - 1) / zc;
+    const long long per_sm = (planes * nch + nsm - 1) / nsm;  // blocks on the busiest SM
+    const double t = (double)per_sm * (zc + 2.0 * (NZT + 1)) / eff(per_sm);  // steps + synchronous prologue
+    if (t < best_t - 1e-9) {
+      best_t = t;
+      best.ZC = zc;
+      best.zchunks = (int)nch;
+    }
+  }
   return best;
 }
 
@@ -109,6 +184,8 @@ struct tp3d_solver {
   bool mixed = false;
   KEP<double> ke64{};
   KEP<float> ke32{};
+  bool ke_cls = false;              // KE has the cubic-symmetry class structure
+  double kcls64[kKEClasses] = {};   // its class values
   double* KE1 = nullptr;
   double penal = 3.0;
   bool have_density = false;
@@ -192,35 +269,42 @@ struct tp3d_solver {
   template <typename T, int MODE>
   int fine(const OpIO<T>& io) {
     const dim3 grid(tile.tiles_y * tile.tiles_x, tile.zchunks);
-    const size_t smem = fine_smem_bytes<T>(tile.TY, tile.TX);
+    int rc;
     if constexpr (sizeof(T) == 8) {
       FineParams<double, EFromF64> p;
       p.ke = ke64;
+      for (int k = 0; k < kKEClasses; ++k) p.kcls[k] = kcls64[k];
       p.g = g;
-      p.TY = tile.TY; p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.mode = MODE;
       p.fix = fix[0];
       p.esrc = EFromF64{E64};
       p.io = io;
-      fine_apply_kernel<double, MODE, EFromF64><<<grid, tile.threads, smem, st>>>(p);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
     } else if (rho16) {
       FineParams<float, EFromBF16> p;
       p.ke = ke32;
+      for (int k = 0; k < kKEClasses; ++k) p.kcls[k] = (float)kcls64[k];
       p.g = g;
-      p.TY = tile.TY; p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.mode = MODE;
       p.fix = fix[0];
       p.esrc = EFromBF16{rho16, (float)penal};
       p.io = io;
-      fine_apply_kernel<float, MODE, EFromBF16><<<grid, tile.threads, smem, st>>>(p);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
     } else {
       FineParams<float, EFromF32> p;
       p.ke = ke32;
+      for (int k = 0; k < kKEClasses; ++k) p.kcls[k] = (float)kcls64[k];
       p.g = g;
-      p.TY = tile.TY; p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.TX = tile.TX; p.ZC = tile.ZC; p.tiles_y = tile.tiles_y; p.tiles_x = tile.tiles_x;
+      p.mode = MODE;
       p.fix = fix[0];
       p.esrc = EFromF32{E32};
       p.io = io;
-      fine_apply_kernel<float, MODE, EFromF32><<<grid, tile.threads, smem, st>>>(p);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
     }
+    if (rc) return rc;
     count_launch();
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
@@ -576,8 +660,41 @@ struct tp3d_solver {
     last_iters = s.iters;
     last_updates = s.updates;
     last_relres = s.bb > 0.0 ? std::sqrt(std::max(s.rr_hi, 0.0) / s.bb) : 0.0;
-    return status_of(s);
+    last_fallback = false;
+    if (s.done == 1 || s.done == 5) return status_of(s);
+    // FP32 could not resolve this system (cap, breakdown, non-finite, or a
+    // stall far above the target): finish it with the FP64 solver.
+    if (int e = ensure_fp64_buffers()) return e;
+    if (s.done == 3 || s.done == 4) TP3D_CHECK(cudaMemsetAsync(u64, 0, ndof * sizeof(double), st));
+    const int mixed_iters = s.iters;
+    last_fallback = true;
+    rc = solve64(F);
+    last_iters += mixed_iters;
+    return rc;
   }
+
+  // FP64 Krylov and level vectors for the mixed form's fallback (allocated on first use).
+  int ensure_fp64_buffers() {
+    if (K64.r) return TP3D_OK;
+    const long long ndof = 3 * g.nnode();
+    K64.u = u64;
+    K64.r = alloc<double>(ndof);
+    K64.p = alloc<double>(ndof);
+    K64.q = alloc<double>(ndof);
+    for (int L = 0; L < nlev; ++L) {
+      const long long n = 3 * grids[L].nnode();
+      auto& a = L64[L];
+      a.x[0] = alloc<double>(n);
+      a.x[1] = alloc<double>(n);
+      a.b = alloc<double>(n);
+      a.r = alloc<double>(n);
+      a.d = alloc<double>(n);
+      if (!a.x[0] || !a.x[1] || !a.b || !a.r || !a.d) return TP3D_ERR_CUDA;
+    }
+    if (!K64.r || !K64.p || !K64.q) return TP3D_ERR_CUDA;
+    return TP3D_OK;
+  }
+  bool last_fallback = false;
 };
 
 // KE1[s] = P_s^T KE P_s: interpolation from a coarse element's corners to its
@@ -660,7 +777,10 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     s->ke64.k[i] = KE_host[i];
     s->ke32.k[i] = (float)KE_host[i];
   }
-  s->tile = choose_tile(s->g, s->nsm);
+  s->ke_cls = ke_classes(KE_host, s->kcls64);
+  s->tile = mixed ? (o.inner_density == 1 ? choose_tile<float, EFromBF16>(s->g, s->nsm)
+                                           : choose_tile<float, EFromF32>(s->g, s->nsm))
+                  : choose_tile<double, EFromF64>(s->g, s->nsm);
   if (s->tile.tiles_y * s->tile.tiles_x * s->tile.zchunks > kMaxPartials)
     return fail(TP3D_ERR_ARG, "grid too large for the partial-sum buffer");
   // levels
@@ -998,7 +1118,7 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
   std::vector<double> v = {(double)s->nlev, (double)s->last_iters, (double)s->last_updates, s->last_relres,
                            (double)s->last_restarts, (double)s->cn, (double)s->tile.TY, (double)s->tile.TX,
                            (double)s->tile.ZC, s->coarse_fallback ? 1.0 : 0.0, lam.empty() ? 0.0 : lam[0],
-                           s->last_floor ? 1.0 : 0.0};
+                           s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

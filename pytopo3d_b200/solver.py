@@ -108,7 +108,8 @@ class HexSolver:
         buf = (C.c_double * 16)()
         n = _lib.lib().tp3d_solver_stats(self._h, buf, 16)
         keys = ["levels", "iterations", "reliable_updates", "relres", "restarts", "coarsest_dofs",
-                "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor"]
+                "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor",
+                "fp64_fallback"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
 
 
