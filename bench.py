@@ -324,7 +324,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": "cantilever 128x64x64, void cylinder r12 (axis y), solid slab x<4, beta 1",
                    "nele": nele, "ndof": ndof, "precision": args.precision, "rmin": RMIN,
-                   "volfrac": VOLFRAC, "l2": "working set (multigrid hierarchy + vectors) > 126 MB L2",
+                   "volfrac": VOLFRAC, "l2": "SIMP step working set (multigrid hierarchy + vectors) > 126 MB L2; roofline kernel timed per launch after a 256 MiB L2 flush",
                    "parallelism": f"replicas x{world}"},
         "dof_cg_iters_per_s": world * ndof * main_r["cg"] / (main_r["ms"] / 1e3),
         "cg_iterations_per_step": main_r["cg"] / steps,

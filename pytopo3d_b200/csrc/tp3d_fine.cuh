@@ -53,16 +53,28 @@ __host__ __device__ constexpr size_t fine_smem_bytes() {
 }
 
 template <typename T>
-__device__ __forceinline__ void fine_epilogue(int mode, const OpIO<T>& io, long long i, bool fx, T kv, T own,
-                                              double& part) {
+__device__ __forceinline__ EpiIn<T> fine_epi_load(int mode, const OpIO<T>& io, long long i) {
   switch (mode) {
-    case kModeApply: op_epilogue<T, kModeApply>(io, i, fx, kv, own, part); break;
-    case kModeResid: op_epilogue<T, kModeResid>(io, i, fx, kv, own, part); break;
-    case kModeJacobi: op_epilogue<T, kModeJacobi>(io, i, fx, kv, own, part); break;
-    case kModeCgQ: op_epilogue<T, kModeCgQ>(io, i, fx, kv, own, part); break;
-    case kModeChebFirst: op_epilogue<T, kModeChebFirst>(io, i, fx, kv, own, part); break;
-    case kModeChebStep: op_epilogue<T, kModeChebStep>(io, i, fx, kv, own, part); break;
-    default: op_epilogue<T, kModeDinvApply>(io, i, fx, kv, own, part); break;
+    case kModeResid: return epi_load<T, kModeResid>(io, i);
+    case kModeJacobi: return epi_load<T, kModeJacobi>(io, i);
+    case kModeChebFirst: return epi_load<T, kModeChebFirst>(io, i);
+    case kModeChebStep: return epi_load<T, kModeChebStep>(io, i);
+    case kModeDinvApply: return epi_load<T, kModeDinvApply>(io, i);
+    default: return EpiIn<T>{};
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void fine_epilogue(int mode, const OpIO<T>& io, long long i, bool fx, T kv, T own,
+                                              const EpiIn<T>& in, double& part) {
+  switch (mode) {
+    case kModeApply: op_epilogue<T, kModeApply>(io, i, fx, kv, own, in, part); break;
+    case kModeResid: op_epilogue<T, kModeResid>(io, i, fx, kv, own, in, part); break;
+    case kModeJacobi: op_epilogue<T, kModeJacobi>(io, i, fx, kv, own, in, part); break;
+    case kModeCgQ: op_epilogue<T, kModeCgQ>(io, i, fx, kv, own, in, part); break;
+    case kModeChebFirst: op_epilogue<T, kModeChebFirst>(io, i, fx, kv, own, in, part); break;
+    case kModeChebStep: op_epilogue<T, kModeChebStep>(io, i, fx, kv, own, in, part); break;
+    default: op_epilogue<T, kModeDinvApply>(io, i, fx, kv, own, in, part); break;
   }
 }
 
@@ -195,6 +207,12 @@ __global__ void __launch_bounds__(256, 2) fine_apply_kernel(const __grid_constan
       for (int j = 0; j < NZT; ++j) {
         const int zn = z + j;
         if (zn < ze) {
+          // epilogue inputs first: their loads overlap the FMAs below
+          const long long n = p.g.nidx(x0 + tx, y0 + ty, zn);
+          const int f = p.fix[n];
+          EpiIn<T> in[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) in[c] = fine_epi_load<T>(p.mode, p.io, 3 * n + c);
           T acc[8][3];
 #pragma unroll
           for (int e = 0; e < 8; ++e)
@@ -246,11 +264,10 @@ __global__ void __launch_bounds__(256, 2) fine_apply_kernel(const __grid_constan
                 for (int c = 0; c < 3; ++c) kv[c] = fma(E, acc[e8][c], kv[c]);
               }
           }
-          const long long n = p.g.nidx(x0 + tx, y0 + ty, zn);
-          const int f = p.fix[n];
           const T* own = su + ((zn + NPL) % NPL) * 3 * PP + toff;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) fine_epilogue<T>(p.mode, p.io, 3 * n + c, (f >> c) & 1, kv[c], own[c * PP], part);
+          for (int c = 0; c < 3; ++c)
+            fine_epilogue<T>(p.mode, p.io, 3 * n + c, (f >> c) & 1, kv[c], own[c * PP], in[c], part);
         }
       }
     }

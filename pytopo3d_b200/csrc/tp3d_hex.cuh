@@ -5,17 +5,15 @@
 // direct / CG solve (pytopo3d/utils/solver.py:15-73).
 //
 // Fine level: y = Z K(E) Z u + (I - Z) u, applied node by node from the 24x24
-// element stiffness KE (kernel-parameter space, i.e. the constant bank, so
-// every FMA takes its coefficient as an immediate-bank operand) and the
-// element moduli E.  Z masks fixed DOFs.  A block owns a TY x TX column of
-// nodes and marches along z; each step stages one new node plane of u (tile +
-// 1 halo) and one element slab of E in shared memory.  Per node the 27
-// neighbours are read once and fed into 8 per-element accumulators (576 FMAs
-// per node, 24 independent FMA chains).
+// element stiffness KE and the element moduli E (kernel in tp3d_fine.cuh).
+// Z masks fixed DOFs.  This file holds what the fine and coarse operators
+// share: modulus sources, the per-DOF epilogues of the smoother / residual /
+// CG modes, the diagonal kernels and the grid transfers.
 //
 // Coarse levels: Galerkin operators P^T A P of the unmasked stiffness with
 // trilinear P, stored as 27-point 3x3-block stencils (243 coefficients per
-// node, structure-of-arrays), fixed DOFs by injection.
+// node, structure-of-arrays) for the hierarchy build, and repacked DOF-major
+// with the coarse fixed DOFs masked out for the apply kernels.
 #pragma once
 
 #include "tp3d_common.cuh"
@@ -80,33 +78,57 @@ __device__ __forceinline__ bool op_skip(const OpIO<T>& io) {
   return (io.done && *(volatile const int*)io.done) || (io.gate && *(volatile const int*)io.gate == 0);
 }
 
+// Per-DOF epilogue inputs, loaded before the operator's FMAs so that their
+// latency overlaps the arithmetic.
+template <typename T>
+struct EpiIn {
+  T b = T(0), dinv = T(0), d = T(0);
+};
+
+template <int MODE>
+__host__ __device__ constexpr bool epi_reads_b() {
+  return MODE == kModeResid || MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep;
+}
+template <int MODE>
+__host__ __device__ constexpr bool epi_reads_dinv() {
+  return MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep || MODE == kModeDinvApply;
+}
+
+template <typename T, int MODE>
+__device__ __forceinline__ EpiIn<T> epi_load(const OpIO<T>& io, long long i) {
+  EpiIn<T> in;
+  if (epi_reads_b<MODE>()) in.b = io.b[i];
+  if (epi_reads_dinv<MODE>()) in.dinv = io.dinv[i];
+  if (MODE == kModeChebStep) in.d = io.d[i];
+  return in;
+}
+
 // Per-DOF epilogue; `own` is this DOF's input value (0 on fixed DOFs).
 template <typename T, int MODE>
-__device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool fx, T kv, T own, double& part) {
+__device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool fx, T kv, T own, const EpiIn<T>& in,
+                                            double& part) {
   if (MODE == kModeApply) {
     io.out[i] = fx ? io.u[i] : kv;
   } else if (MODE == kModeResid) {
-    io.out[i] = fx ? T(0) : io.b[i] - kv;
+    io.out[i] = fx ? T(0) : in.b - kv;
   } else if (MODE == kModeJacobi) {
-    io.out[i] = fx ? T(0) : own + io.omega * io.dinv[i] * (io.b[i] - kv);
+    io.out[i] = fx ? T(0) : own + io.omega * in.dinv * (in.b - kv);
   } else if (MODE == kModeCgQ) {
     const T q = fx ? T(0) : kv;
     io.out[i] = q;
     part += (double)own * (double)q;
   } else if (MODE == kModeChebFirst) {
-    const T dd = fx ? T(0) : (T)io.coef[0] * io.dinv[i] * (io.b[i] - kv);
+    const T dd = fx ? T(0) : (T)io.coef[0] * in.dinv * (in.b - kv);
     io.d[i] = dd;
     io.out[i] = own + dd;
   } else if (MODE == kModeChebStep) {
-    const T dd = fx ? T(0)
-                    : (T)io.coef[2 * io.step] * io.d[i] + (T)io.coef[2 * io.step + 1] * io.dinv[i] * (io.b[i] - kv);
+    const T dd = fx ? T(0) : (T)io.coef[2 * io.step] * in.d + (T)io.coef[2 * io.step + 1] * in.dinv * (in.b - kv);
     io.d[i] = dd;
     io.out[i] = own + dd;
   } else {  // kModeDinvApply
-    io.out[i] = fx ? T(0) : io.dinv[i] * kv;
+    io.out[i] = fx ? T(0) : in.dinv * kv;
   }
 }
-
 
 // Diagonal of the fine operator: D[n,c] = sum_e E_e KE[3a+c][3a+c]; 1 on fixed DOFs.
 // Writes its inverse.
@@ -147,54 +169,87 @@ __global__ void fine_diag_inv_kernel(Grid g, const __grid_constant__ KEP<double>
 __host__ __device__ constexpr int stencil_k(int jrel, int c, int d) { return (jrel * 3 + c) * 3 + d; }
 __host__ __device__ constexpr int jrel_of(int dx, int dy, int dz) { return (dz + 1) * 9 + (dx + 1) * 3 + (dy + 1); }
 
+// Apply layout ("packed"): S[(jrel * 3 + d) * ndof + 3 n + c] = A[(n,c),(m,d)]
+// with m = n + offset(jrel), set to zero wherever DOF (n,c) or (m,d) is fixed
+// or m lies outside the grid.  One thread owns one DOF, so every coefficient
+// load of a warp is one contiguous run, and the masking needs no mask loads
+// for the neighbours.
+template <typename T>
+__global__ void stencil_pack_kernel(Grid g, const double* __restrict__ A, const uint8_t* __restrict__ fix, T* S) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const long long nn = g.nnode(), ndof = 3 * nn;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x) {
+    const long long n = i / 3;
+    const int c = (int)(i - 3 * n);
+    const int iy = (int)(n % NY);
+    const long long r = n / NY;
+    const int ix = (int)(r % NX), iz = (int)(r / NX);
+    const bool fi = (fix[n] >> c) & 1;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int x = ix + dx, y = iy + dy, z = iz + dz;
+          const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
+          const int fm = in ? fix[g.nidx(x, y, z)] : 7;
+          const int jr = jrel_of(dx, dy, dz);
+          for (int d = 0; d < 3; ++d) {
+            const double v = (fi || ((fm >> d) & 1)) ? 0.0 : A[(long long)stencil_k(jr, c, d) * nn + n];
+            S[(long long)(jr * 3 + d) * ndof + i] = (T)v;
+          }
+        }
+  }
+}
+
 template <typename T>
 struct StencilParams {
   Grid g;
-  const T* A;
+  const T* S;  // packed layout
   const uint8_t* fix;
   OpIO<T> io;
 };
 
+// One DOF per thread: 81 coalesced coefficient loads and 81 neighbour loads,
+// all independent (offsets past the grid are clamped to the node itself and
+// meet a zero coefficient), so a thread waits for memory about once.  Coarse
+// levels hold far fewer than 2^31 DOFs: 32-bit index arithmetic.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T> p) {
   if (op_skip(p.io)) return;
   __shared__ double red[32];
   const Grid g = p.g;
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
-  const long long nn = g.nnode();
-  const T* __restrict__ A = p.A;
+  const int NXY = NX * NY;
+  const int ndof = 3 * NXY * NZ;
+  const T* __restrict__ S = p.S;
   const T* __restrict__ u = p.io.u;
   double part = 0.0;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(n % NY);
-    const long long r = n / NY;
-    const int ix = (int)(r % NX), iz = (int)(r / NX);
-    T kv[3] = {T(0), T(0), T(0)};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ndof; i += gridDim.x * blockDim.x) {
+    const int n = i / 3, c = i - 3 * n;
+    const int iy = n % NY, r = n / NY;
+    const int ix = r % NX, iz = r / NX;
+    const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
+    const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
+    const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
+    T kv = T(0);
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+    for (int a = 0; a < 3; ++a) {
+      const int oz = a == 0 ? oz0 : (a == 1 ? 0 : oz2);
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx)
+      for (int b = 0; b < 3; ++b) {
+        const int ox = b == 0 ? ox0 : (b == 1 ? 0 : ox2);
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const int x = ix + dx, y = iy + dy, z = iz + dz;
-          if (x < 0 || x >= NX || y < 0 || y >= NY || z < 0 || z >= NZ) continue;
-          const long long m = g.nidx(x, y, z);
-          const int fm = p.fix[m];
-          const int jr = jrel_of(dx, dy, dz);
-          T um[3];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) um[d] = ((fm >> d) & 1) ? T(0) : __ldg(&u[3 * m + d]);
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) kv[c] = fma(__ldg(&A[(long long)stencil_k(jr, c, d) * nn + n]), um[d], kv[c]);
+        for (int e = 0; e < 3; ++e) {
+          const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
+          const int m3 = 3 * (n + oz + ox + oy);
+          const T* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
+          kv = fma(__ldg(s), __ldg(&u[m3]), kv);
+          kv = fma(__ldg(s + ndof), __ldg(&u[m3 + 1]), kv);
+          kv = fma(__ldg(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
         }
-    const int f = p.fix[n];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const bool fx = (f >> c) & 1;
-      op_epilogue<T, MODE>(p.io, 3 * n + c, fx, kv[c], fx ? T(0) : u[3 * n + c], part);
+      }
     }
+    const bool fx = (p.fix[n] >> c) & 1;
+    op_epilogue<T, MODE>(p.io, i, fx, kv, fx ? T(0) : u[i], epi_load<T, MODE>(p.io, i), part);
   }
   if (MODE == kModeCgQ) {
     part = block_sum(part, red);
@@ -238,66 +293,93 @@ __host__ __device__ inline Grid coarse_grid(const Grid& f) {
   return Grid{(f.nx + 1) / 2, (f.ny + 1) / 2, (f.nz + 1) / 2};
 }
 
-// b_c[I] = sum_i P[i,I] r_f[i], 0 on fixed coarse DOFs.
+// Grid transfers run one thread per node of an (x, y) plane, blockIdx.y = z
+// (one integer division per thread), and handle the node's three components.
+inline dim3 plane_grid(int nxy, int nz) { return dim3((unsigned)((nxy + 255) / 256), (unsigned)nz); }
+
+// b_c[I] = sum_i P[i,I] r_f[i], 0 on fixed coarse DOFs.  The 27 fine
+// neighbours are read unconditionally (offsets past the fine grid are clamped
+// and weighted 0), so the loads are independent.  Grid: plane_grid(CX*CY, CZ).
 template <typename T>
-__global__ void restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf, const uint8_t* __restrict__ fixc, T* bc,
-                                const int* done) {
+__global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf,
+                                                       const uint8_t* __restrict__ fixc, T* bc, const int* done) {
   if (done && *(volatile const int*)done) return;
   const int FX = gf.nx + 1, FY = gf.ny + 1, FZ = gf.nz + 1;
   const int CX = gc.nx + 1, CY = gc.ny + 1;
-  const long long nn = gc.nnode();
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
-    const int Iy = (int)(n % CY);
-    const long long r = n / CY;
-    const int Ix = (int)(r % CX), Iz = (int)(r / CX);
-    T s[3] = {T(0), T(0), T(0)};
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= CX * CY) return;
+  const int Iz = blockIdx.y, Ix = t / CY, Iy = t - Ix * CY;
+  const int FXY = FX * FY;
+  T s0 = T(0), s1 = T(0), s2 = T(0);
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = 2 * Iz + dz;
+    const bool vz = z >= 0 && z < FZ;
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx)
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = 2 * Ix + dx;
+      const bool vx = x >= 0 && x < FX;
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy) {
-          const int x = 2 * Ix + dx, y = 2 * Iy + dy, z = 2 * Iz + dz;
-          if (x < 0 || x >= FX || y < 0 || y >= FY || z < 0 || z >= FZ) continue;
-          const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
-          const long long m = gf.nidx(x, y, z);
-#pragma unroll
-          for (int c = 0; c < 3; ++c) s[c] = fma(w, rf[3 * m + c], s[c]);
-        }
-    const int f = fixc[n];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) bc[3 * n + c] = ((f >> c) & 1) ? T(0) : s[c];
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = 2 * Iy + dy;
+        const bool v = vz && vx && y >= 0 && y < FY;
+        const T w = v ? T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0)) : T(0);
+        const T* src = rf + 3 * (v ? y + FY * x + FXY * z : 0);
+        s0 = fma(w, __ldg(src), s0);
+        s1 = fma(w, __ldg(src + 1), s1);
+        s2 = fma(w, __ldg(src + 2), s2);
+      }
+    }
   }
+  const long long n = t + (long long)CX * CY * Iz;
+  const int f = fixc[n];
+  T* dst = bc + 3 * n;
+  dst[0] = (f & 1) ? T(0) : s0;
+  dst[1] = (f & 2) ? T(0) : s1;
+  dst[2] = (f & 4) ? T(0) : s2;
 }
 
-// x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.
+// x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.  A fine node takes 1, 2, 4
+// or 8 coarse nodes (weights 1 or 1/2 per axis), read as a fixed 2x2x2 block
+// with zero weights for the absent ones.  Grid: plane_grid(FX*FY, FZ).
 template <typename T>
-__global__ void prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc, const uint8_t* __restrict__ fixf,
-                                   T* xf, const int* done) {
+__global__ void __launch_bounds__(256) prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc,
+                                                          const uint8_t* __restrict__ fixf, T* xf, const int* done) {
   if (done && *(volatile const int*)done) return;
   const int FX = gf.nx + 1, FY = gf.ny + 1;
-  const long long nn = gf.nnode();
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
-    const int iy = (int)(n % FY);
-    const long long r = n / FY;
-    const int ix = (int)(r % FX), iz = (int)(r / FX);
-    T s[3] = {T(0), T(0), T(0)};
-    const int nxp = (ix & 1) ? 2 : 1, nyp = (iy & 1) ? 2 : 1, nzp = (iz & 1) ? 2 : 1;
-    const T wx = (ix & 1) ? T(0.5) : T(1), wy = (iy & 1) ? T(0.5) : T(1), wz = (iz & 1) ? T(0.5) : T(1);
-    for (int a = 0; a < nzp; ++a)
-      for (int b = 0; b < nxp; ++b)
-        for (int c2 = 0; c2 < nyp; ++c2) {
-          const int Ix = (ix >> 1) + b, Iy = (iy >> 1) + c2, Iz = (iz >> 1) + a;
-          const long long m = gc.nidx(Ix, Iy, Iz);
-          const T w = wx * wy * wz;
+  const int CX = gc.nx + 1, CY = gc.ny + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= FX * FY) return;
+  const int iz = blockIdx.y, ix = t / FY, iy = t - ix * FY;
+  const long long n = t + (long long)FX * FY * iz;
+  const int f = fixf[n];
+  if (f == 7) return;
+  const int oy = iy & 1, ox = ix & 1, oz = iz & 1;
+  const int CXY = CX * CY;
+  const int base = (iy >> 1) + CY * (ix >> 1) + CXY * (iz >> 1);
+  const T h = T(0.5);
+  T s0 = T(0), s1 = T(0), s2 = T(0);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) s[c] = fma(w, xc[3 * m + c], s[c]);
-        }
-    const int f = fixf[n];
+  for (int a = 0; a < 2; ++a) {
+    const T wz = oz ? h : (a ? T(0) : T(1));
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if (!((f >> c) & 1)) xf[3 * n + c] += s[c];
+    for (int b = 0; b < 2; ++b) {
+      const T wx = ox ? h : (b ? T(0) : T(1));
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const T wy = oy ? h : (e ? T(0) : T(1));
+        const T w = wz * wx * wy;
+        const T* src = xc + 3 * (base + (e & oy) + CY * (b & ox) + CXY * (a & oz));
+        s0 = fma(w, __ldg(src), s0);
+        s1 = fma(w, __ldg(src + 1), s1);
+        s2 = fma(w, __ldg(src + 2), s2);
+      }
+    }
   }
+  T* dst = xf + 3 * n;
+  if (!(f & 1)) dst[0] += s0;
+  if (!(f & 2)) dst[1] += s1;
+  if (!(f & 4)) dst[2] += s2;
 }
 
 }  // namespace tp3d

@@ -260,6 +260,7 @@ __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const dou
   __shared__ int bad;
   __shared__ double piv;
   const long long nn = (long long)n * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   for (long long t = threadIdx.x; t < nn; t += blockDim.x) A[t] = D[t];
   if (threadIdx.x == 0) bad = 0;
   __syncthreads();
@@ -271,10 +272,14 @@ __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const dou
     }
     __syncthreads();
     const double pk = piv;
-    // entries off row k and column k, from the old row/column
-    for (long long t = threadIdx.x; t < nn; t += blockDim.x) {
-      const int i = (int)(t / n), j = (int)(t % n);
-      if (i != k && j != k) A[t] -= A[(size_t)i * n + k] * A[(size_t)k * n + j] * pk;
+    // entries off row k and column k, from the old row/column: a warp per row
+    for (int i = warp; i < n; i += nwarps) {
+      if (i == k) continue;
+      double* Ai = A + (size_t)i * n;
+      const double f = Ai[k] * pk;
+      const double* Ak = A + (size_t)k * n;
+      for (int j = lane; j < n; j += 32)
+        if (j != k) Ai[j] -= f * Ak[j];
     }
     __syncthreads();
     for (int t = threadIdx.x; t < n; t += blockDim.x) {

@@ -44,25 +44,58 @@ struct OcArgs {
   GridBarrier bar;
 };
 
-__device__ __forceinline__ bool is_free(const OcArgs& a, long long e) {
-  return !((a.solid && a.solid[e]) || (a.vd && a.vd[e]));
+// Per-element code written once per call into the ratio scratch: for a free
+// element q = sqrt(normalised ratio) >= 0; -1 marks protected solid, -2
+// protected void (void wins where both are set, as in the reference).
+constexpr double kCodeSolid = -1.0, kCodeVoid = -2.0;
+
+// Candidate value (oc_update.py:76-91): x sqrt(max(r / (lam + 1e-30), 1e-30))
+// = x max(q / sqrt(lam + 1e-30), 1e-15), then the move limit and [0, 1].
+// `isl` = 1 / sqrt(lam + 1e-30), uniform over the launch.
+__device__ __forceinline__ double candidate_q(double xe, double q, double isl, double move) {
+  if (q < 0.0) return q == kCodeSolid ? 1.0 : 0.0;
+  double c = xe * fmax(q * isl, 1e-15);
+  c = fmax(xe - move, fmin(xe + move, c));
+  return fmin(fmax(c, 0.0), 1.0);
 }
 
-// Candidate value (oc_update.py:76-91): free elements move toward
-// x sqrt(ratio / lambda) within the move limit; protected ones are clamped.
-__device__ __forceinline__ double candidate(const OcArgs& a, long long e, double lam) {
-  const bool so = a.solid && a.solid[e], vo = a.vd && a.vd[e];
-  const double xe = __ldg(&a.x[e]);
-  double v = xe;
-  if (!so && !vo) {
-    const double r = fmax(__ldg(&a.ratio[e]) / (lam + 1e-30), 1e-30);
-    double c = xe * sqrt(r);
-    c = fmax(xe - a.move, fmin(xe + a.move, c));
-    v = fmin(fmax(c, 0.0), 1.0);
+// Projected free volume of the candidate at multiplier lam (oc_update.py:78-111):
+// stage candidates of each owned tile (+ halo), filter, project, sum; per-block
+// partials go to `part`, and after the grid barrier every block sums them in the
+// same order.  Returns false if the barrier wait expired.  (Arrays written
+// earlier in this launch are read through L2, __ldcg, never the L1 path.)
+template <int Z>
+__device__ bool oc_volume(const OcArgs& a, double lam, double* part, double* s, double* red, double* vol) {
+  constexpr int SY = kFilterTY + 2 * Z, SX = kFilterTX + 2 * Z, SZ = kFilterKZ + 2 * Z;
+  constexpr int NS = SY * SX * SZ;
+  const long long ntiles = filter_ntiles(a.g);
+  const double isl = 1.0 / sqrt(lam + 1e-30);
+  double vpart = 0.0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const FilterTile tile = filter_tile_at(a.g, t);
+    __syncthreads();
+#pragma unroll 4
+    for (int i = threadIdx.x; i < NS; i += kFilterThreads) {
+      const int ly = i % SY, r = i / SY;
+      const int lx = r % SX, lz = r / SX;
+      const int gx = tile.x0 + lx - Z, gy = tile.y0 + ly - Z, gz = tile.z0 + lz - Z;
+      double v = 0.0;
+      if (gx >= 0 && gx < a.g.nx && gy >= 0 && gy < a.g.ny && gz >= 0 && gz < a.g.nz) {
+        const long long e = a.g.eidx(gx, gy, gz);
+        v = candidate_q(__ldg(&a.x[e]), __ldcg(&a.ratio[e]), isl, a.move);
+      }
+      s[i] = v;
+    }
+    __syncthreads();
+    filter_apply<Z>(a.g, a.fc, tile, s, [&](long long e, int, int, int, double v) {
+      if (__ldcg(&a.ratio[e]) >= 0.0) vpart += a.pr.value(v / __ldg(&a.Hs[e]), nullptr);
+    });
   }
-  if (so) v = 1.0;
-  if (vo) v = 0.0;
-  return v;
+  vpart = block_sum(vpart, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = vpart;
+  if (!grid_sync(a.bar)) return false;
+  *vol = sum_partials(part, gridDim.x, red);
+  return true;
 }
 
 template <int Z>
@@ -72,11 +105,13 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   const long long ntiles = filter_ntiles(a.g);
   const long long nele = a.g.nele();
   const int nblk = gridDim.x;
+  auto solid_at = [&](long long e) { return a.solid && a.solid[e]; };
+  auto void_at = [&](long long e) { return a.vd && a.vd[e]; };
 
   // ---- ratio normalisation (oc_update.py:54-68) ----
   double m = 0.0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nele; e += (long long)nblk * blockDim.x) {
-    if (is_free(a, e)) {
+    if (!solid_at(e) && !void_at(e)) {
       const double r = fmax(-__ldg(&a.dc[e]) / fmax(__ldg(&a.dv[e]), 1e-20), 0.0);
       a.ratio[e] = r;
       m = fmax(m, r);
@@ -92,31 +127,29 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
     scale = block_max(t, red);
   }
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nele; e += (long long)nblk * blockDim.x) {
-    if (is_free(a, e)) a.ratio[e] = scale > 0.0 ? a.ratio[e] / scale : 1.0;
+    double q;
+    if (void_at(e)) q = kCodeVoid;
+    else if (solid_at(e)) q = kCodeSolid;
+    else q = sqrt(scale > 0.0 ? a.ratio[e] / scale : 1.0);
+    a.ratio[e] = q;
   }
   if (!grid_sync(a.bar)) return;
 
   // ---- bisection (oc_update.py:70-122) ----
+  // The reference starts from [0, 1e12]; while the projected volume stays at or
+  // below the target it only halves the upper bound, so its first midpoints are
+  // 1e12 / 2^j, j = 1, 2, ...  The volume does not increase with the
+  // multiplier, so the number K of such steps is found by a binary search over
+  // j, and steps 1..K need no evaluation of their own: the smallest volume
+  // error among them is that of step K (volume closest to the target from
+  // below).  Steps K + 1 onwards are the reference's ordinary bisection.  (A
+  // tolerance of 1 or more would end the reference's loop after one step; the
+  // search is skipped then.)
   double lo = 0.0, hi = 1.0e12;
   double best_err = INFINITY, best_lam = NAN, best_vol = NAN;
-  int it = 0;
-  for (; it < a.max_iter; ++it) {
-    const double lam = 0.5 * (lo + hi);
-    double vpart = 0.0;
-    for (long long t = blockIdx.x; t < ntiles; t += nblk) {
-      const FilterTile tile = filter_tile_at(a.g, t);
-      __syncthreads();
-      filter_stage<Z>(a.g, tile, s, [&](long long e, int, int, int) { return candidate(a, e, lam); });
-      __syncthreads();
-      filter_apply<Z>(a.g, a.fc, tile, s, [&](long long e, int, int, int, double v) {
-        if (is_free(a, e)) vpart += a.pr.value(v / __ldg(&a.Hs[e]), nullptr);
-      });
-    }
-    vpart = block_sum(vpart, red);
-    double* part = (it & 1) ? a.partB : a.partA;
-    if (threadIdx.x == 0) part[blockIdx.x] = vpart;
-    if (!grid_sync(a.bar)) return;
-    const double vol = sum_partials(part, nblk, red);
+  int it = 0, pass = 0;
+  bool done = false;
+  auto record = [&](double lam, double vol) {
     const double err = fabs(vol - a.target);
     if (err < best_err) {
       best_err = err;
@@ -125,19 +158,49 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
     }
     if (vol > a.target) lo = lam;
     else hi = lam;
-    if ((hi - lo) / fmax(hi + lo, DBL_MIN) < a.tol) {
-      ++it;
-      break;
+    ++it;
+    if ((hi - lo) / fmax(hi + lo, DBL_MIN) < a.tol) done = true;
+  };
+  if (a.tol < 1.0) {
+    int jlo = 0, jhi = a.max_iter + 1;
+    double vlo = NAN, vhi = NAN;
+    bool first = true;  // probe j = 1 first: it is the reference's own first step, and K = 0 is common
+    while (jhi - jlo > 1) {
+      const int jm = first ? 1 : (jlo + jhi) >> 1;
+      first = false;
+      double v;
+      if (!oc_volume<Z>(a, ldexp(1.0e12, -jm), (pass++ & 1) ? a.partB : a.partA, s, red, &v)) return;
+      if (v > a.target) {
+        jhi = jm;
+        vhi = v;
+      } else {
+        jlo = jm;
+        vlo = v;
+      }
     }
+    if (jlo >= 1) {  // steps 1..jlo: only the best of them (step jlo) is recorded
+      it = jlo - 1;
+      hi = ldexp(1.0e12, -(jlo - 1));
+      record(ldexp(1.0e12, -jlo), vlo);
+    }
+    if (jhi <= a.max_iter && !done) record(ldexp(1.0e12, -jhi), vhi);  // = 0.5 (lo + hi)
+  }
+  while (!done && it < a.max_iter) {
+    const double lam = 0.5 * (lo + hi);
+    double vol;
+    if (!oc_volume<Z>(a, lam, (pass++ & 1) ? a.partB : a.partA, s, red, &vol)) return;
+    record(lam, vol);
   }
 
   // ---- best candidate, its density, and change (optimizer.py:642) ----
   const bool have = !isnan(best_lam);
+  const double isl = have ? 1.0 / sqrt(best_lam + 1e-30) : 0.0;
   double cmax = 0.0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nele; e += (long long)nblk * blockDim.x) {
-    const double v = have ? candidate(a, e, best_lam) : __ldg(&a.x[e]);
+    const double xe = __ldg(&a.x[e]), q = a.ratio[e];
+    const double v = have ? candidate_q(xe, q, isl, a.move) : xe;
     a.x_new[e] = v;
-    if (is_free(a, e)) cmax = fmax(cmax, fabs(v - __ldg(&a.x[e])));
+    if (q >= 0.0) cmax = fmax(cmax, fabs(v - xe));
   }
   cmax = block_max(cmax, red);
   if (threadIdx.x == 0) a.partC[blockIdx.x] = cmax;
@@ -145,12 +208,13 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   for (long long t = blockIdx.x; t < ntiles; t += nblk) {
     const FilterTile tile = filter_tile_at(a.g, t);
     __syncthreads();
-    filter_stage<Z>(a.g, tile, s, [&](long long e, int, int, int) { return a.x_new[e]; });
+    filter_stage<Z>(a.g, tile, s, [&](long long e, int, int, int) { return __ldcg(&a.x_new[e]); });
     __syncthreads();
     filter_apply<Z>(a.g, a.fc, tile, s, [&](long long e, int, int, int, double v) {
       double r = a.pr.value(v / __ldg(&a.Hs[e]), nullptr);
-      if (a.solid && a.solid[e]) r = 1.0;
-      if (a.vd && a.vd[e]) r = 0.0;
+      const double q = __ldcg(&a.ratio[e]);
+      if (q == kCodeSolid) r = 1.0;
+      if (q == kCodeVoid) r = 0.0;
       a.rho_new[e] = r;
     });
   }

@@ -258,7 +258,8 @@ __global__ void dense_diag_inverse_kernel(int n, const double* __restrict__ Dori
 }
 
 // Deterministic pseudo-random start vector on free DOFs (power iteration).
-__global__ void random_vector_kernel(long long nn, const uint8_t* __restrict__ fix, double* v) {
+template <typename T>
+__global__ void random_vector_kernel(long long nn, const uint8_t* __restrict__ fix, T* v) {
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
     const int f = fix[n];
 #pragma unroll
@@ -268,7 +269,7 @@ __global__ void random_vector_kernel(long long nn, const uint8_t* __restrict__ f
       h *= 0xBF58476D1CE4E5B9ull;
       h ^= h >> 32;
       const double r = 2.0 * (double)(h >> 11) * (1.0 / 9007199254740992.0) - 1.0;  // [-1, 1)
-      v[3 * n + c] = ((f >> c) & 1) ? 0.0 : r;
+      v[3 * n + c] = ((f >> c) & 1) ? T(0) : (T)r;
     }
   }
 }
@@ -304,11 +305,12 @@ __global__ void cheb_setup_kernel(const double* __restrict__ pa, int na, const d
 }
 
 // dst = src * (*scale)
-__global__ void scale_copy_kernel(long long n, const double* __restrict__ src, const double* __restrict__ scale,
+template <typename T>
+__global__ void scale_copy_kernel(long long n, const T* __restrict__ src, const double* __restrict__ scale,
                                   double* dst) {
   const double s = *scale;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = src[i] * s;
+    dst[i] = (double)src[i] * s;
 }
 
 }  // namespace tp3d

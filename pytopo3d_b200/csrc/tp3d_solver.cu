@@ -46,7 +46,7 @@ struct LevelVec {
   T* r = nullptr;
   T* d = nullptr;  // Chebyshev direction
   T* dinv = nullptr;
-  T* A = nullptr;  // stencil (levels >= 1)
+  T* A = nullptr;  // packed stencil for the apply kernels (levels >= 1)
 };
 
 template <typename T>
@@ -316,10 +316,10 @@ struct tp3d_solver {
     if (L == 0) return fine<T, MODE>(io);
     StencilParams<T> p;
     p.g = grids[L];
-    p.A = levels<T>()[L].A;
+    p.S = levels<T>()[L].A;
     p.fix = fix[L];
     p.io = io;
-    stencil_apply_kernel<T, MODE><<<grid_blocks(grids[L].nnode()), 256, 0, st>>>(p);
+    stencil_apply_kernel<T, MODE><<<grid_blocks(3 * grids[L].nnode()), 256, 0, st>>>(p);
     count_launch();
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
@@ -384,11 +384,13 @@ struct tp3d_solver {
       *rc |= apply_level<T, kModeResid>(L, io);
     }
     auto& lc = levels<T>()[L + 1];
-    restrict_kernel<T><<<grid_blocks(grids[L + 1].nnode()), 256, 0, st>>>(gl, grids[L + 1], lv.r, fix[L + 1], lc.b,
+    const Grid& gn = grids[L + 1];
+    restrict_kernel<T><<<plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), 256, 0, st>>>(gl, gn, lv.r, fix[L + 1], lc.b,
                                                                            done);
     count_launch();
     T* xc = vcycle<T>(L + 1, lc.b, done, rc);
-    prolong_add_kernel<T><<<grid_blocks(gl.nnode()), 256, 0, st>>>(gl, grids[L + 1], xc, fix[L], lv.x[cur], done);
+    prolong_add_kernel<T><<<plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1), 256, 0, st>>>(gl, gn, xc, fix[L],
+                                                                                             lv.x[cur], done);
     count_launch();
     *rc |= smooth_steps<T>(L, 0, o.post_sweeps, &cur, b, done);
     if (cudaGetLastError() != cudaSuccess) *rc = TP3D_ERR_CUDA;
@@ -690,11 +692,25 @@ struct tp3d_solver {
       a.r = alloc<double>(n);
       a.d = alloc<double>(n);
       if (!a.x[0] || !a.x[1] || !a.b || !a.r || !a.d) return TP3D_ERR_CUDA;
+      if (L > 0) {
+        a.A = alloc<double>(243 * grids[L].nnode());
+        if (!a.A) return TP3D_ERR_CUDA;
+        pack_level<double>(L, a.A);
+      }
     }
     if (!K64.r || !K64.p || !K64.q) return TP3D_ERR_CUDA;
+    TP3D_CHECK_LAUNCH();
     return TP3D_OK;
   }
+
+  // Packed (apply-layout) copy of the level-L stencil.
+  template <typename T>
+  void pack_level(int L, T* S) {
+    stencil_pack_kernel<T><<<grid_blocks(3 * grids[L].nnode()), 256, 0, st>>>(grids[L], A64[L], fix[L], S);
+    count_launch();
+  }
   bool last_fallback = false;
+  unsigned char* flush = nullptr;  // L2 flush buffer of tp3d_solver_time_apply
 };
 
 // KE1[s] = P_s^T KE P_s: interpolation from a coarse element's corners to its
@@ -834,9 +850,9 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     if (L > 0) s->A64[L] = s->alloc<double>(243 * nn);
     s->coef.push_back(s->alloc<double>(kCoefLen));
     auto& a = s->L64[L];
-    a.dinv = s->alloc<double>(ndof);  // FP64 diagonal: power iteration in both forms
-    a.A = s->A64[L];
+    a.dinv = s->alloc<double>(ndof);  // FP64 diagonal (the mixed form rounds it)
     if (!mixed) {
+      if (L > 0) a.A = s->alloc<double>(243 * nn);
       a.x[0] = s->alloc<double>(ndof); a.x[1] = s->alloc<double>(ndof);
       a.b = s->alloc<double>(ndof); a.r = s->alloc<double>(ndof); a.d = s->alloc<double>(ndof);
     } else {
@@ -886,10 +902,13 @@ extern "C" int tp3d_solver_destroy(tp3d_solver* s) {
   return TP3D_OK;
 }
 
-// lambda_max(Dinv A) per level by power iteration (FP64 operators), then the
-// Chebyshev coefficients; all on the device.  The first call starts from a
-// pseudo-random vector; later calls start from the previous (normalised)
-// dominant vector, which tracks the slowly changing design in fewer steps.
+// lambda_max(Dinv A) per level by power iteration, then the Chebyshev
+// coefficients; all on the device.  The operators are those of the solve's
+// own precision (FP32 in the mixed form: two digits of lambda_max suffice).
+// The first call starts from a pseudo-random vector; later calls start from
+// the previous (normalised) dominant vector, which tracks the slowly changing
+// design in fewer steps.
+template <typename T>
 static int estimate_spectra(tp3d_solver* s) {
   cudaStream_t st = s->st;
   const bool warm = s->have_spectra;
@@ -897,27 +916,41 @@ static int estimate_spectra(tp3d_solver* s) {
   for (int L = 0; L < s->nlev - (s->nlev > 1 ? 1 : 0); ++L) {
     const long long nn = s->grids[L].nnode(), ndof = 3 * nn;
     const int nb = s->grid_blocks(ndof);
-    if (warm) {
-      TP3D_CHECK(cudaMemcpyAsync(s->pw[0], s->pv[L], ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    auto& lv = s->levels<T>()[L];
+    T* w[2];
+    if constexpr (sizeof(T) == 8) {
+      w[0] = s->pw[0];
+      w[1] = s->pw[1];
     } else {
-      random_vector_kernel<<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->fix[L], s->pw[0]);
+      w[0] = lv.x[0];
+      w[1] = lv.x[1];
+    }
+    if (warm) {
+      if constexpr (sizeof(T) == 8) {
+        TP3D_CHECK(cudaMemcpyAsync(w[0], s->pv[L], ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      } else {
+        convert_kernel<double, T><<<nb, 256, 0, st>>>(ndof, s->pv[L], w[0]);
+        count_launch();
+      }
+    } else {
+      random_vector_kernel<T><<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->fix[L], w[0]);
       count_launch();
     }
     int cur = 0;
     for (int k = 0; k < N; ++k) {
-      OpIO<double> io;
-      io.u = s->pw[cur];
-      io.out = s->pw[1 - cur];
-      io.dinv = s->L64[L].dinv;
-      if (int rc = s->apply_level<double, kModeDinvApply>(L, io)) return rc;
+      OpIO<T> io;
+      io.u = w[cur];
+      io.out = w[1 - cur];
+      io.dinv = lv.dinv;
+      if (int rc = s->apply_level<T, kModeDinvApply>(L, io)) return rc;
       cur = 1 - cur;
     }
-    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, s->pw[cur], s->pw[cur], s->partials, nullptr, nullptr);
-    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, s->pw[1 - cur], s->pw[1 - cur], s->partials + kMaxPartials / 2,
-                                           nullptr, nullptr);
+    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], w[cur], s->partials, nullptr, nullptr);
+    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[1 - cur], w[1 - cur], s->partials + kMaxPartials / 2, nullptr,
+                                      nullptr);
     cheb_setup_kernel<<<1, 256, 0, st>>>(s->partials, nb, s->partials + kMaxPartials / 2, nb, s->o.cheb_ratio,
                                          1.1, s->coef[L]);
-    scale_copy_kernel<<<nb, 256, 0, st>>>(ndof, s->pw[cur], s->coef[L] + kCoefLen - 1, s->pv[L]);
+    scale_copy_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], s->coef[L] + kCoefLen - 1, s->pv[L]);
     for (int i = 0; i < 4; ++i) count_launch();
     TP3D_CHECK_LAUNCH();
   }
@@ -962,10 +995,10 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     count_launch();
     if (mixed) {
       convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
-      convert_kernel<double, float><<<s->grid_blocks(243 * nn), 256, 0, st>>>(243 * nn, s->A64[L], s->L32[L].A);
       count_launch();
-      count_launch();
+      s->pack_level<float>(L, s->L32[L].A);
     }
+    if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // FP64 form, or the mixed form's fallback
     TP3D_CHECK_LAUNCH();
   }
   if (s->nlev > 1) {
@@ -1022,7 +1055,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     }
   }
   if (s->o.smoother != 1)
-    if (int rc = estimate_spectra(s)) return rc;
+    if (int rc = mixed ? estimate_spectra<float>(s) : estimate_spectra<double>(s)) return rc;
   TP3D_CHECK_LAUNCH();
   s->have_density = true;
   return s->leave();
@@ -1071,37 +1104,42 @@ extern "C" int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y) {
   return s->leave();
 }
 
+// Average duration of one fine-operator launch (Apply mode) with a cold L2:
+// a 256 MiB buffer is written between launches and each launch is bracketed
+// by its own pair of events on the solver's stream.
 extern "C" int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch) {
   if (!s || !ms_per_launch || launches < 1 || !s->have_density) return TP3D_ERR_ARG;
   if (fp32 && !s->mixed) return TP3D_ERR_ARG;
+  constexpr size_t kFlushBytes = (size_t)256 << 20;
+  if (!s->flush) s->flush = s->alloc<unsigned char>(kFlushBytes);
+  if (!s->flush) return TP3D_ERR_CUDA;
   if (int rc = s->enter()) return rc;
   cudaEvent_t a, b;
   TP3D_CHECK(cudaEventCreate(&a));
   TP3D_CHECK(cudaEventCreate(&b));
   int rc = TP3D_OK;
-  auto run = [&]() {
-    for (int i = 0; i < launches && rc == TP3D_OK; ++i) {
-      if (fp32) {
-        OpIO<float> io;
-        io.u = s->K32.p;
-        io.out = s->K32.q;
-        rc = s->fine<float, kModeApply>(io);
-      } else {
-        OpIO<double> io;
-        io.u = s->u64;
-        io.out = s->pw[0];
-        rc = s->fine<double, kModeApply>(io);
-      }
+  double total = 0.0;
+  for (int i = -1; i < launches && rc == TP3D_OK; ++i) {  // i = -1: warm-up
+    TP3D_CHECK(cudaMemsetAsync(s->flush, i & 0xff, kFlushBytes, s->st));
+    TP3D_CHECK(cudaEventRecord(a, s->st));
+    if (fp32) {
+      OpIO<float> io;
+      io.u = s->K32.p;
+      io.out = s->K32.q;
+      rc = s->fine<float, kModeApply>(io);
+    } else {
+      OpIO<double> io;
+      io.u = s->u64;
+      io.out = s->pw[0];
+      rc = s->fine<double, kModeApply>(io);
     }
-  };
-  run();  // warm-up
-  TP3D_CHECK(cudaEventRecord(a, s->st));
-  run();
-  TP3D_CHECK(cudaEventRecord(b, s->st));
-  TP3D_CHECK(cudaEventSynchronize(b));
-  float ms = 0.f;
-  TP3D_CHECK(cudaEventElapsedTime(&ms, a, b));
-  *ms_per_launch = ms / launches;
+    TP3D_CHECK(cudaEventRecord(b, s->st));
+    TP3D_CHECK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    TP3D_CHECK(cudaEventElapsedTime(&ms, a, b));
+    if (i >= 0) total += ms;
+  }
+  *ms_per_launch = total / launches;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (rc) return rc;

@@ -206,3 +206,45 @@ def test_oc_rejects_bad_arguments(P):
     with pytest.raises(ValueError):
         P.optimality_criteria_update_projected(z, z, z, 0.2, 1.0, H, Hs, 1.0, 0.5, ~m, m, m,
                                                max_bisection_iterations=0)
+
+
+def _oracle_bisection(tag_inputs, max_iter, tol):
+    """(steps, best lambda, final lo, final hi) of the reference bisection, replayed from the oracle trace."""
+    x, dc, dv, move, target, H, Hs, beta, eta, free, solid, void = tag_inputs
+    trace = []
+    O.oc_update_projected(x, dc, dv, move, target, H, Hs, beta, eta, free, solid, void,
+                          max_bisection_iterations=max_iter, bisection_tolerance=tol, trace=trace)
+    lo, hi, best, best_err = 0.0, 1.0e12, None, float("inf")
+    for lam, vol in trace:
+        err = abs(vol - target)
+        if err < best_err:
+            best, best_err = lam, err
+        if vol > target:
+            lo = lam
+        else:
+            hi = lam
+    return len(trace), best, lo, hi
+
+
+@pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
+@pytest.mark.parametrize("max_iter,tol", [(80, 1e-8), (30, 1e-8), (12, 1e-8), (80, 1e-3), (80, 1.5)])
+def test_oc_bisection_path_matches_reference(P, golden, tag, max_iter, tol):
+    # the multiplier sequence is exact binary fractions of 1e12: same path, same numbers
+    from pytopo3d_b200.oc_update import OCWorkspace, oc_update_flat
+    from pytopo3d_b200._tensors import to_flat, to_flat_mask, vec
+
+    nx, ny, nz, volfrac, penal, rmin, beta, eta, move, _ = golden[f"it{tag}_dims"]
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    solid, void = golden[f"it{tag}_solid"], golden[f"it{tag}_void"]
+    x, dc, dv = golden[f"it{tag}_x"], golden[f"it{tag}_dc_dx"], golden[f"it{tag}_dv_dx"]
+    target = float(golden[f"it{tag}_target"])
+    Ho, Hso = O.build_filter(nx, ny, nz, rmin)
+    steps, best, lo, hi = _oracle_bisection((x, dc, dv, move, target, Ho, Hso, beta, eta, ~(solid | void), solid,
+                                             void), max_iter, tol)
+    H, Hs = P.build_filter(nx, ny, nz, rmin)
+    xf = to_flat(x)
+    xn, rn = torch.empty_like(xf), torch.empty_like(xf)
+    st = oc_update_flat(H, xf, to_flat(dc), to_flat(dv), vec(Hs), to_flat_mask(solid), to_flat_mask(void), move,
+                        target, beta, eta, xn, rn, OCWorkspace(H), max_iter, tol).cpu().numpy()
+    assert int(st[2]) == steps
+    assert st[0] == best and st[5] == lo and st[6] == hi
