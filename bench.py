@@ -113,13 +113,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_loop(precision, x0=None):
+def make_loop(precision, x0=None, solver_options=None):
     from pytopo3d_b200.optimizer import SimpLoop
     from pytopo3d_b200.stiffness import lk_H8
 
     shape, solid, void, F, fixed = workload(NELX, NELY, NELZ)
     loop = SimpLoop(NELX, NELY, NELZ, VOLFRAC, PENAL, RMIN, lk_H8(elem_size=1.0), F, fixed, solid, void,
-                    projection_eta=ETA, move=MOVE, precision=precision, x0=x0)
+                    projection_eta=ETA, move=MOVE, precision=precision, x0=x0, solver_options=solver_options)
     loop.set_beta(BETA)
     return loop
 
@@ -228,6 +228,8 @@ def main():
                     help="step: warm-up + --steps loop bodies only (for launch lists); "
                          "apply: fine-operator launches only (for kernel captures)")
     ap.add_argument("--size", type=int, default=NELX, help="nelx for --mode step/apply (nely = nelz = nelx/2)")
+    ap.add_argument("--fine-operator", type=int, default=0,
+                    help="solver option fine_operator for --mode step/apply (0 timed choice)")
     args = ap.parse_args()
     if args.mode != "bench":
         return run_probe(args)
@@ -301,11 +303,13 @@ def main():
     alg_bytes = (8 * ndof + 2 * nele) if fp32 else (16 * ndof + 8 * nele)
     achieved = alg_bytes / (main_r["apply_ms"] * 1e-3) / 1e9
     flops = 1152.0 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
+    form = main_r["stats"].get("fine_form_fp32" if fp32 else "fine_form_fp64", 0)
+    kname = "wht_apply" if form and form >= 1 else "fine_apply"
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("fine_apply_" + ("f32" if fp32 else "f64"))
+            traffic = json.load(open(tf)).get(kname + ("_f32" if fp32 else "_f64"))
         except Exception:
             traffic = None
 
@@ -335,7 +339,7 @@ def main():
                                 "apply_ms": results[p]["apply_ms"]} for p in other},
         "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": 8 * nele,
                 "d2h_bytes_per_step": 8 * nele + 8},
-        "roofline": {"bound": "hbm", "kernel": "fine_apply_kernel<" + ("float" if fp32 else "double") + ">",
+        "roofline": {"bound": "hbm", "kernel": kname + "_kernel<" + ("float" if fp32 else "double") + ">",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic, "bytes_per_launch": alg_bytes,
                      "launch_ms": main_r["apply_ms"],
@@ -359,7 +363,7 @@ def run_probe(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     NELX, NELY, NELZ = args.size, args.size // 2, args.size // 2
-    loop = make_loop(args.precision)
+    loop = make_loop(args.precision, solver_options={"fine_operator": args.fine_operator})
     if args.mode == "step":
         for _ in range(max(1, args.warmup)):
             loop.step()
@@ -375,7 +379,7 @@ def run_probe(args):
         loop.solver.set_density(loop.S.rho_p, PENAL)
         ms = ctypes_time_apply(loop.solver, fp32=(args.precision == "mixed"))
         print(json.dumps({"mode": "apply", "size": [NELX, NELY, NELZ], "precision": args.precision,
-                          "apply_ms": ms}))
+                          "apply_ms": ms, "solver": loop.solver.stats()}))
     loop.close()
     return 0
 

@@ -153,6 +153,11 @@ typedef struct tp3d_solver_opts {
   int inner_density;    /* mixed: FP32 fine operator from 0 = FP32 moduli, 1 = BF16 densities */
   double reliable_delta;/* mixed: replace the FP32 residual by the FP64 one when it fell by this factor */
   int max_restarts;     /* FP64: restarts from the true residual when the recursive one drifted */
+  int fine_operator;    /* fine-level K u: 0 the fastest of the dense-KE form and the Walsh-Hadamard
+                           block form's launch shapes, timed on the grid at the first set_density;
+                           1 dense KE; 2 Walsh-Hadamard (fastest shape); 3, 4, 5 Walsh-Hadamard with
+                           shape 0, 1, 2.  The block form needs an axis-aligned orthotropic KE and
+                           falls back to the dense form otherwise. */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -187,8 +192,11 @@ int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
  * for the roofline figure; no reference counterpart. */
 int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch);
 
-/* Diagnostics of the last solve: [levels, iterations, refinements, relres,
- * inner_iterations_total, coarsest_dofs, ...]; returns the count written. */
+/* Diagnostics of the last solve, in this order: levels, CG iterations, reliable updates
+ * (mixed), relres, restarts (FP64), coarsest dense size, dense-form tile (y, x, z chunk),
+ * coarsest-inverse fallback flag, lambda_max(Dinv A) of the fine level, residual-floor flag,
+ * FP64-fallback flag (mixed), fine form of the FP64 operator and of the FP32 operator
+ * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent).  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 #ifdef __cplusplus

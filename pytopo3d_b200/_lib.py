@@ -47,6 +47,7 @@ class SolverOpts(C.Structure):
         ("inner_density", i32),
         ("reliable_delta", f64),
         ("max_restarts", i32),
+        ("fine_operator", i32),
     ]
 
 

@@ -1,0 +1,191 @@
+// Launch side of the Walsh-Hadamard fine operator (tp3d_fine_wht.cuh):
+// explicit instantiations per precision, modulus source, epilogue mode and
+// block shape; the KE block split; the tile chooser.
+#include <algorithm>
+#include <cmath>
+
+#include "tp3d_fine_wht.cuh"
+
+namespace tp3d {
+
+namespace {
+
+// (threads, min blocks per SM) of each variant, per precision
+template <typename T>
+struct WhtShapes;
+template <>
+struct WhtShapes<float> {
+  static constexpr int nthr[kWhtVariants] = {512, 768, 256};
+  static constexpr int minb[kWhtVariants] = {2, 1, 4};
+};
+template <>
+struct WhtShapes<double> {
+  static constexpr int nthr[kWhtVariants] = {256, 384, 128};
+  static constexpr int minb[kWhtVariants] = {2, 1, 4};
+};
+
+template <typename T, class ESrc, int V>
+struct WhtVariant {
+  static constexpr int NTHR = WhtShapes<T>::nthr[V];
+  static constexpr int MINB = WhtShapes<T>::minb[V];
+  template <int MODE>
+  static void* fn() {
+    return (void*)wht_apply_kernel<T, ESrc, MODE, NTHR, MINB>;
+  }
+  static void* by_mode(int mode) {
+    switch (mode) {
+      case kModeApply: return fn<kModeApply>();
+      case kModeResid: return fn<kModeResid>();
+      case kModeJacobi: return fn<kModeJacobi>();
+      case kModeCgQ: return fn<kModeCgQ>();
+      case kModeChebFirst: return fn<kModeChebFirst>();
+      case kModeChebStep: return fn<kModeChebStep>();
+      default: return fn<kModeDinvApply>();
+    }
+  }
+};
+
+template <typename T, class ESrc>
+void* wht_fn(int mode, int v) {
+  switch (v) {
+    case 0: return WhtVariant<T, ESrc, 0>::by_mode(mode);
+    case 1: return WhtVariant<T, ESrc, 1>::by_mode(mode);
+    default: return WhtVariant<T, ESrc, 2>::by_mode(mode);
+  }
+}
+
+// dynamic shared memory of every instantiation raised once to what it needs
+template <typename T, class ESrc>
+bool wht_prepare(int v) {
+  static bool done[kWhtVariants] = {};
+  if (done[v]) return true;
+  const int nthr = WhtShapes<T>::nthr[v];
+  const int smem = (int)wht_smem_bytes<T>(nthr);
+  for (int mode = 0; mode <= kModeDinvApply; ++mode)
+    if (cudaFuncSetAttribute(wht_fn<T, ESrc>(mode, v), cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+      return false;
+  done[v] = true;
+  return true;
+}
+
+}  // namespace
+
+template <typename T, class ESrc>
+int wht_variant_threads(int v) {
+  return WhtShapes<T>::nthr[v];
+}
+
+template <typename T, class ESrc>
+int wht_occupancy(int v) {
+  if (!wht_prepare<T, ESrc>(v)) return 1;
+  int occ = 0;
+  const int nthr = WhtShapes<T>::nthr[v];
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wht_fn<T, ESrc>(kModeChebStep, v), nthr,
+                                                wht_smem_bytes<T>(nthr));
+  return std::max(occ, 1);
+}
+
+template <typename T, class ESrc>
+int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st) {
+  if (v < 0 || v >= kWhtVariants || !wht_prepare<T, ESrc>(v)) return TP3D_ERR_ARG;
+  const int nthr = WhtShapes<T>::nthr[v];
+  void* args[] = {(void*)&p};
+  const cudaError_t e = cudaLaunchKernel(wht_fn<T, ESrc>(mode, v), grid, dim3(nthr), args,
+                                         wht_smem_bytes<T>(nthr), st);
+  return e == cudaSuccess ? TP3D_OK : TP3D_ERR_CUDA;
+}
+
+bool wht_blocks_from_ke(const double* KE, double m[8][3][3]) {
+  // W[(s, i), (a, i)] = (-1)^(s . offset(a)), s = sx + 2 sy + 4 sz
+  auto sgn = [](int s, int a) {
+    const int d = (s & 1) * corner_ox(a) + ((s >> 1) & 1) * corner_oy(a) + ((s >> 2) & 1) * corner_oz(a);
+    return (d & 1) ? -1.0 : 1.0;
+  };
+  double mx = 0.0;
+  for (int i = 0; i < 576; ++i) mx = std::max(mx, std::fabs(KE[i]));
+  if (!(mx > 0.0)) return false;
+  // Mfull = W KE W^T / 64
+  static double Mf[24][24];
+  for (int s1 = 0; s1 < 8; ++s1)
+    for (int i = 0; i < 3; ++i)
+      for (int s2 = 0; s2 < 8; ++s2)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0;
+          for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) acc += sgn(s1, a) * sgn(s2, b) * KE[(3 * a + i) * 24 + 3 * b + j];
+          Mf[3 * s1 + i][3 * s2 + j] = acc / 64.0;
+        }
+  const double tol = 1e-12 * mx;
+  for (int s1 = 0; s1 < 8; ++s1)
+    for (int i = 0; i < 3; ++i)
+      for (int s2 = 0; s2 < 8; ++s2)
+        for (int j = 0; j < 3; ++j) {
+          const bool in_block = (s1 ^ (1 << i)) == (s2 ^ (1 << j));
+          const bool translation = s1 == 0 || s2 == 0;
+          if ((!in_block || translation) && std::fabs(Mf[3 * s1 + i][3 * s2 + j]) > tol) return false;
+        }
+  for (int t = 0; t < 8; ++t)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) m[t][i][j] = Mf[3 * (t ^ (1 << i)) + i][3 * (t ^ (1 << j)) + j];
+  return true;
+}
+
+// The patch is PY = TY + 2 threads along y (the contiguous direction) by
+// TX + 2 along x; the tile with the fewest blocks per node plane wins (ties:
+// the larger tile).  Then the number of z chunks that minimises the busiest
+// SM's work, counting each block's prologue as 1.5 planes and crediting
+// co-resident blocks for hiding each other's barrier and memory latency.
+template <typename T, class ESrc>
+WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  WhtTile best;
+  best.variant = v;
+  best.nthr = WhtShapes<T>::nthr[v];
+  long long best_blocks = -1;
+  for (int PY = 4; PY <= std::min(best.nthr / 4, NY + 2); ++PY) {
+    const int TY = PY - 2;
+    const int TX = best.nthr / PY - 2;
+    if (TX < 2) continue;
+    const long long ky = (NY + TY - 1) / TY, kx = (NX + TX - 1) / TX;
+    const long long blocks = ky * kx;
+    if (best_blocks < 0 || blocks < best_blocks || (blocks == best_blocks && TX * TY > best.TX * best.TY)) {
+      best_blocks = blocks;
+      best.TX = TX;
+      best.TY = TY;
+      best.PY = PY;
+      best.tiles_y = (int)ky;
+      best.tiles_x = (int)kx;
+    }
+  }
+  best.occ = wht_occupancy<T, ESrc>(v);
+  auto eff = [&](long long L) {
+    const long long l = std::min<long long>(L, best.occ);
+    return l <= 1 ? 1.0 : (l == 2 ? 1.6 : (l == 3 ? 1.85 : 2.0));
+  };
+  double best_t = 1e300;
+  for (int zc = 1; zc <= NZ; ++zc) {
+    const long long nch = (NZ + zc - 1) / zc;
+    if ((nch - 1) * zc >= NZ) continue;
+    const long long per_sm = (best_blocks * nch + nsm - 1) / nsm;
+    const double t = (double)per_sm * (zc + 1.5) / eff(per_sm);
+    if (t < best_t - 1e-9) {
+      best_t = t;
+      best.ZC = zc;
+      best.zchunks = (int)nch;
+    }
+  }
+  return best;
+}
+
+#define TP3D_WHT_INSTANTIATE(T, ESrc)                                                     \
+  template int wht_variant_threads<T, ESrc>(int);                                        \
+  template int wht_occupancy<T, ESrc>(int);                                              \
+  template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t); \
+  template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);
+TP3D_WHT_INSTANTIATE(double, EFromF64)
+TP3D_WHT_INSTANTIATE(float, EFromF32)
+TP3D_WHT_INSTANTIATE(float, EFromBF16)
+#undef TP3D_WHT_INSTANTIATE
+
+}  // namespace tp3d

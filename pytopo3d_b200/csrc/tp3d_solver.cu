@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "tp3d_fine.cuh"
+#include "tp3d_fine_wht.cuh"
 #include "tp3d_pcg.cuh"
 
 namespace tp3d {
@@ -220,6 +221,14 @@ struct tp3d_solver {
   PcgState* state = nullptr;
   PcgState* state_host = nullptr;  // two pinned slots
   Tile tile;
+  // Walsh-Hadamard form of the fine operator (used when KE allows it and the
+  // timed choice at the first set_density prefers it), per precision
+  bool wht_ok = false;
+  WhtBlocks<double> wb64{};
+  WhtBlocks<float> wb32{};
+  WhtTile wt64, wt32;
+  bool use_wht64 = false, use_wht32 = false;
+  bool fine_chosen = false;
   std::vector<void*> allocs;
 
   int last_iters = 0, last_updates = 0, last_restarts = 0;
@@ -268,6 +277,7 @@ struct tp3d_solver {
   // ---------------- operators ----------------
   template <typename T, int MODE>
   int fine(const OpIO<T>& io) {
+    if (use_wht<T>()) return fine_wht<T>(MODE, io);
     const dim3 grid(tile.tiles_y * tile.tiles_x, tile.zchunks);
     int rc;
     if constexpr (sizeof(T) == 8) {
@@ -309,7 +319,128 @@ struct tp3d_solver {
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
   }
-  int fine_partials() const { return tile.tiles_y * tile.tiles_x * tile.zchunks; }
+  template <typename T>
+  bool use_wht() const {
+    if constexpr (sizeof(T) == 8) return use_wht64;
+    else return use_wht32;
+  }
+  template <typename T>
+  const WhtTile& wtile() const {
+    if constexpr (sizeof(T) == 8) return wt64;
+    else return wt32;
+  }
+  template <typename T, class ESrc>
+  int wht_launch_with(int mode, const OpIO<T>& io, const WhtTile& w, ESrc esrc) {
+    WhtParams<T, ESrc> p;
+    if constexpr (sizeof(T) == 8) p.mb = wb64;
+    else p.mb = wb32;
+    p.g = g;
+    p.TX = w.TX; p.TY = w.TY; p.PY = w.PY; p.ZC = w.ZC;
+    p.tiles_y = w.tiles_y; p.tiles_x = w.tiles_x;
+    p.fix = fix[0];
+    p.esrc = esrc;
+    p.io = io;
+    return wht_launch<T, ESrc>(p, mode, w.variant, dim3(w.tiles_y * w.tiles_x, w.zchunks), st);
+  }
+  template <typename T>
+  int fine_wht_tile(int mode, const OpIO<T>& io, const WhtTile& w) {
+    int rc;
+    if constexpr (sizeof(T) == 8) rc = wht_launch_with<double>(mode, io, w, EFromF64{E64});
+    else if (rho16) rc = wht_launch_with<float>(mode, io, w, EFromBF16{rho16, (float)penal});
+    else rc = wht_launch_with<float>(mode, io, w, EFromF32{E32});
+    if (rc) {
+      tp3d_set_last_error("fine operator launch failed");
+      return rc;
+    }
+    count_launch();
+    TP3D_CHECK_LAUNCH();
+    return TP3D_OK;
+  }
+  template <typename T>
+  int fine_wht(int mode, const OpIO<T>& io) {
+    return fine_wht_tile<T>(mode, io, wtile<T>());
+  }
+  // Fine operator form for precision T: the dense-KE kernel or one of the
+  // Walsh-Hadamard variants, whichever runs the Apply mode fastest on this
+  // grid (2 warm-up and 6 timed launches each, events on the solver stream);
+  // fine_operator = 1 / 2 restricts the choice to one form.
+  template <typename T>
+  int choose_fine_form() {
+    bool& use = sizeof(T) == 8 ? use_wht64 : use_wht32;
+    WhtTile& wt = sizeof(T) == 8 ? wt64 : wt32;
+    use = false;
+    if (!wht_ok) return TP3D_OK;
+    const T* in;
+    T* out;
+    if constexpr (sizeof(T) == 8) {
+      in = u64;
+      out = pw[0];
+    } else {
+      in = K32.p;
+      out = K32.q;
+    }
+    TP3D_CHECK(cudaMemsetAsync((void*)in, 0, 3 * g.nnode() * sizeof(T), st));
+    cudaEvent_t a, b;
+    TP3D_CHECK(cudaEventCreate(&a));
+    TP3D_CHECK(cudaEventCreate(&b));
+    auto time_one = [&](double* ms) -> int {
+      OpIO<T> io;
+      io.u = in;
+      io.out = out;
+      for (int i = 0; i < 2; ++i)
+        if (int rc = fine<T, kModeApply>(io)) return rc;
+      TP3D_CHECK(cudaEventRecord(a, st));
+      for (int i = 0; i < 6; ++i)
+        if (int rc = fine<T, kModeApply>(io)) return rc;
+      TP3D_CHECK(cudaEventRecord(b, st));
+      TP3D_CHECK(cudaEventSynchronize(b));
+      float f = 0.f;
+      TP3D_CHECK(cudaEventElapsedTime(&f, a, b));
+      *ms = f;
+      return TP3D_OK;
+    };
+    double best = 1e300;
+    int best_v = -1;
+    int rc = TP3D_OK;
+    if (o.fine_operator == 0) rc = time_one(&best);  // dense form
+    for (int v = 0; v < kWhtVariants && rc == TP3D_OK; ++v) {
+      if (o.fine_operator > 2 && v != o.fine_operator - 3) continue;
+      WhtTile w;
+      if constexpr (sizeof(T) == 8) w = wht_choose_tile<double, EFromF64>(g, nsm, v);
+      else if (rho16) w = wht_choose_tile<float, EFromBF16>(g, nsm, v);
+      else w = wht_choose_tile<float, EFromF32>(g, nsm, v);
+      if ((long long)w.tiles_y * w.tiles_x * w.zchunks > kMaxPartials) continue;
+      wt = w;
+      use = true;
+      double ms = 0.0;
+      rc = time_one(&ms);
+      use = false;
+      if (rc == TP3D_OK && ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (best_v >= 0) {
+      if constexpr (sizeof(T) == 8) wt = wht_choose_tile<double, EFromF64>(g, nsm, best_v);
+      else if (rho16) wt = wht_choose_tile<float, EFromBF16>(g, nsm, best_v);
+      else wt = wht_choose_tile<float, EFromF32>(g, nsm, best_v);
+      use = true;
+    }
+    return TP3D_OK;
+  }
+
+  template <typename T>
+  int fine_partials() const {
+    if (use_wht<T>()) {
+      const WhtTile& w = wtile<T>();
+      return w.tiles_y * w.tiles_x * w.zchunks;
+    }
+    return tile.tiles_y * tile.tiles_x * tile.zchunks;
+  }
+
 
   template <typename T, int MODE>
   int apply_level(int L, const OpIO<T>& io) {
@@ -480,7 +611,7 @@ struct tp3d_solver {
     io.partials = partials;
     io.done = done;
     int rc = fine<double, kModeCgQ>(io);
-    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials(), state, kFinPQ, 0.0, nullptr); count_launch();
+    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials<double>(), state, kFinPQ, 0.0, nullptr); count_launch();
     cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials); count_launch();
     finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRR, 0.0, nullptr); count_launch();
     double* z = vcycle<double>(0, K.r, done, &rc);
@@ -597,7 +728,7 @@ struct tp3d_solver {
     io.partials = partials;
     io.done = done;
     int rc = fine<float, kModeCgQ>(io);
-    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials(), state, kFinPQMixed, 0.0, nullptr);
+    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials<float>(), state, kFinPQMixed, 0.0, nullptr);
     count_launch();
     cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials); count_launch();
     finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRMixed, 0.0, nullptr); count_launch();
@@ -758,6 +889,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->inner_density = 0;
   o->reliable_delta = 0.05;
   o->max_restarts = 3;
+  o->fine_operator = 0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -794,6 +926,18 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     s->ke32.k[i] = (float)KE_host[i];
   }
   s->ke_cls = ke_classes(KE_host, s->kcls64);
+  if (o.fine_operator < 0 || o.fine_operator > 2 + kWhtVariants)
+    return fail(TP3D_ERR_ARG, "invalid fine_operator option");
+  {
+    double m[8][3][3];
+    s->wht_ok = o.fine_operator != 1 && wht_blocks_from_ke(KE_host, m);
+    for (int t = 0; t < 8; ++t)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          s->wb64.m[t][i][j] = s->wht_ok ? m[t][i][j] : 0.0;
+          s->wb32.m[t][i][j] = (float)s->wb64.m[t][i][j];
+        }
+  }
   s->tile = mixed ? (o.inner_density == 1 ? choose_tile<float, EFromBF16>(s->g, s->nsm)
                                            : choose_tile<float, EFromF32>(s->g, s->nsm))
                   : choose_tile<double, EFromF64>(s->g, s->nsm);
@@ -980,6 +1124,12 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     count_launch();
   }
   TP3D_CHECK_LAUNCH();
+  if (!s->fine_chosen) {
+    if (int rc = s->choose_fine_form<double>()) return rc;
+    if (mixed)
+      if (int rc = s->choose_fine_form<float>()) return rc;
+    s->fine_chosen = true;
+  }
   for (int L = 1; L < s->nlev; ++L) {
     const Grid& gf = s->grids[L - 1];
     const Grid& gc = s->grids[L];
@@ -1156,7 +1306,9 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
   std::vector<double> v = {(double)s->nlev, (double)s->last_iters, (double)s->last_updates, s->last_relres,
                            (double)s->last_restarts, (double)s->cn, (double)s->tile.TY, (double)s->tile.TX,
                            (double)s->tile.ZC, s->coarse_fallback ? 1.0 : 0.0, lam.empty() ? 0.0 : lam[0],
-                           s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0};
+                           s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0,
+                           s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
+                           s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -41,8 +41,12 @@ def _oracle_apply(rho, KE, penal, nx, ny, nz, fmask, u):
     return z * (K @ (z * u)) + fmask * u
 
 
-@pytest.mark.parametrize("dims", [(6, 4, 3), (5, 7, 2), (1, 1, 1), (13, 3, 4), (8, 33, 3)])
-def test_apply_matches_assembled_matrix(P, dims):
+# fine_operator 1: dense-KE kernel; 2: Walsh-Hadamard block kernel.  The
+# larger grids span several tiles in x and y and several z chunks.
+@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("dims", [(6, 4, 3), (5, 7, 2), (1, 1, 1), (13, 3, 4), (8, 33, 3), (41, 70, 9),
+                                  (70, 9, 41)])
+def test_apply_matches_assembled_matrix(P, dims, form):
     from pytopo3d_b200._tensors import to_flat
     from pytopo3d_b200.solver import HexSolver
 
@@ -52,8 +56,10 @@ def test_apply_matches_assembled_matrix(P, dims):
     u = np.random.default_rng(1).normal(size=fmask.size)
     y_ref = _oracle_apply(rho, KE, 3.0, nx, ny, nz, fmask, u)
     for prec in ("fp64", "mixed"):
-        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec)
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, fine_operator=form)
         s.set_density(to_flat(rho), 3.0)
+        st = s.stats()
+        assert (st["fine_form_fp64"] == 0) if form == 1 else (st["fine_form_fp64"] >= 1)
         y = s.apply(torch.as_tensor(u).cuda()).cpu().numpy()
         np.testing.assert_allclose(y, y_ref, rtol=0, atol=1e-13 * np.abs(y_ref).max())
         if prec == "mixed":
@@ -64,7 +70,7 @@ def test_apply_matches_assembled_matrix(P, dims):
             np.testing.assert_allclose(y32, y32_ref, rtol=0, atol=2e-6 * np.abs(y32_ref).max())
         s.close()
     # BF16-density FP32 operator against the operator of the rounded densities
-    s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", inner_density=1)
+    s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", inner_density=1, fine_operator=form)
     s.set_density(to_flat(rho), 3.0)
     rho16 = torch.as_tensor(rho).to(torch.bfloat16).double().numpy()
     y16_ref = _oracle_apply(rho16, KE, 3.0, nx, ny, nz, fmask, u.astype(np.float32).astype(float))
