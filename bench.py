@@ -148,6 +148,33 @@ def time_device_steps(loop, steps, dist):
     return ms, cg, launches, c
 
 
+def accuracy_vs_fp64(loop, precision):
+    """Relative compliance (u'Ku) and displacement errors of one solve of the
+    loop's own solver on its current design and warm start, against an FP64
+    solve of the same system to relative residual 1e-12 (or its floor)."""
+    from pytopo3d_b200.solver import HexSolver
+    from pytopo3d_b200.stiffness import lk_H8
+
+    S = loop.S
+    rho, F, U0 = S.rho_p.clone(), S.F[0], S.U[0].clone()
+    fixed = workload(NELX, NELY, NELZ)[4]
+    ref = HexSolver(NELX, NELY, NELZ, lk_H8(elem_size=1.0), fixed, precision="fp64", rtol=1e-12,
+                    max_iterations=10000)
+    ref.set_density(rho, PENAL)
+    Ur = ref.solve(F, U0.clone(), raise_on_fail=False)
+    loop.solver.set_density(rho, PENAL)
+    Um = loop.solver.solve(F, U0.clone())
+    c_r = float(Ur @ ref.apply(Ur))
+    c_m = float(Um @ ref.apply(Um))
+    out = {"precision": precision, "rtol": loop.solver.opts.rtol, "iterations": loop.solver.last_iterations,
+           "compliance_rel_err": abs(c_m - c_r) / abs(c_r),
+           "displacement_rel_err": float((Um - Ur).norm() / Ur.norm()),
+           "reference": {"precision": "fp64", "rtol": 1e-12, "relres": ref.last_relres,
+                         "iterations": ref.last_iterations}}
+    ref.close()
+    return out
+
+
 def barrier(dist):
     if dist is not None:
         dist.barrier()
@@ -230,6 +257,8 @@ def main():
     ap.add_argument("--size", type=int, default=NELX, help="nelx for --mode step/apply (nely = nelz = nelx/2)")
     ap.add_argument("--fine-operator", type=int, default=0,
                     help="solver option fine_operator for --mode step/apply (0 timed choice)")
+    ap.add_argument("--solver-opt", action="append", default=[], metavar="KEY=VALUE",
+                    help="further solver options for --mode step/apply (integers or floats)")
     args = ap.parse_args()
     if args.mode != "bench":
         return run_probe(args)
@@ -273,6 +302,7 @@ def main():
         apply_ms = (ctypes_time_apply(loop.solver, fp32=(prec == "mixed")))
         results[prec] = dict(ms=ms, steps=steps, cg=cg, launches=launches, c=c, apply_ms=apply_ms,
                              loop=loop, stats=loop.solver.stats())
+        results[prec]["accuracy"] = accuracy_vs_fp64(loop, prec)
         if prec != args.precision:
             loop.close()
 
@@ -334,9 +364,12 @@ def main():
         "cg_iterations_per_step": main_r["cg"] / steps,
         "compliance": main_r["c"],
         "solver": {k: v for k, v in main_r["stats"].items()},
+        "accuracy_vs_fp64": main_r["accuracy"],
         "other_precision": {p: {"value": world * results[p]["steps"] / (results[p]["ms"] / 1e3),
+                                "ms_per_step": results[p]["ms"] / results[p]["steps"],
                                 "cg_iterations_per_step": results[p]["cg"] / results[p]["steps"],
-                                "apply_ms": results[p]["apply_ms"]} for p in other},
+                                "apply_ms": results[p]["apply_ms"], "accuracy_vs_fp64": results[p]["accuracy"]}
+                            for p in other},
         "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": 8 * nele,
                 "d2h_bytes_per_step": 8 * nele + 8},
         "roofline": {"bound": "hbm", "kernel": kname + "_kernel<" + ("float" if fp32 else "double") + ">",
@@ -363,7 +396,11 @@ def run_probe(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     NELX, NELY, NELZ = args.size, args.size // 2, args.size // 2
-    loop = make_loop(args.precision, solver_options={"fine_operator": args.fine_operator})
+    opts = {"fine_operator": args.fine_operator}
+    for kv in args.solver_opt:
+        k, v = kv.split("=", 1)
+        opts[k] = float(v) if any(ch in v for ch in ".e") else int(v)
+    loop = make_loop(args.precision, solver_options=opts)
     if args.mode == "step":
         for _ in range(max(1, args.warmup)):
             loop.step()

@@ -158,6 +158,13 @@ typedef struct tp3d_solver_opts {
                            1 dense KE; 2 Walsh-Hadamard (fastest shape); 3, 4, 5 Walsh-Hadamard with
                            shape 0, 1, 2.  The block form needs an axis-aligned orthotropic KE and
                            falls back to the dense form otherwise. */
+  int fused_cycle_dofs; /* the V-cycle from the first level (>= 1) with at most this many DOFs down
+                           to the coarsest runs as one cooperative launch with grid barriers;
+                           0 (default) keeps one launch per smoothing step and transfer, which
+                           measured faster inside the CUDA graph of a CG iteration on B200 */
+  int galerkin;         /* levels >= 2: 0 (default) element-wise Galerkin products (level-2 element
+                           matrices from the fine moduli, deeper ones from their 8 sub-elements,
+                           then assembled to stencils); 1 stencil triple product P^T A P */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -196,7 +203,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * (mixed), relres, restarts (FP64), coarsest dense size, dense-form tile (y, x, z chunk),
  * coarsest-inverse fallback flag, lambda_max(Dinv A) of the fine level, residual-floor flag,
  * FP64-fallback flag (mixed), fine form of the FP64 operator and of the FP32 operator
- * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent).  Returns the count written. */
+ * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent), first level of the fused
+ * coarse cycle (0 none).  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 #ifdef __cplusplus

@@ -48,6 +48,8 @@ class SolverOpts(C.Structure):
         ("reliable_delta", f64),
         ("max_restarts", i32),
         ("fine_operator", i32),
+        ("fused_cycle_dofs", i32),
+        ("galerkin", i32),
     ]
 
 

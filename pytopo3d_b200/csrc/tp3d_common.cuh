@@ -137,6 +137,37 @@ __device__ __forceinline__ bool grid_sync(GridBarrier b) {
   return s_ok != 0;
 }
 
+// Grid-wide barrier with one atomic per block: block 0 adds 2^31 - (nblocks - 1),
+// every other block adds 1, so the top bit of the word flips exactly when the
+// last block arrives, and each block waits for the flip of the value it saw.
+// The word returns to its low bits after every barrier, so it needs no reset
+// between barriers or launches (only a zero before the first launch, and
+// after an expired wait).  Bounded like grid_sync: after kSpinLimit polls the
+// wait raises *err and returns false.
+__device__ __forceinline__ bool grid_sync_flip(unsigned int* word, int* err) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    const unsigned int nblk = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int inc = (blockIdx.x | blockIdx.y | blockIdx.z) == 0 ? 0x80000000u - (nblk - 1) : 1u;
+    __threadfence();
+    const unsigned int seen = atomicAdd(word, inc);
+    int ok = 1;
+    long long spins = 0;
+    while (((seen ^ *(volatile unsigned int*)word) & 0x80000000u) == 0) {
+      if (++spins > kSpinLimit || *(volatile int*)err != 0) {
+        atomicExch(err, TP3D_ERR_TIMEOUT);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? TP3D_OK : TP3D_ERR_CUDA; }
 
 // Process-wide count of kernel launches issued by this library (graph

@@ -212,42 +212,51 @@ struct StencilParams {
 // all independent (offsets past the grid are clamped to the node itself and
 // meet a zero coefficient), so a thread waits for memory about once.  Coarse
 // levels hold far fewer than 2^31 DOFs: 32-bit index arithmetic.
+// Row i of the packed stencil times u (K u at DOF i; fixed rows and columns are
+// zero in the packed layout).
+template <typename T>
+__device__ __forceinline__ T stencil_row(const Grid& g, const T* __restrict__ S, const T* __restrict__ u, int i) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const int NXY = NX * NY;
+  const int ndof = 3 * NXY * NZ;
+  const int n = i / 3;
+  const int iy = n % NY, r = n / NY;
+  const int ix = r % NX, iz = r / NX;
+  const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
+  const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
+  const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
+  T kv = T(0);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int oz = a == 0 ? oz0 : (a == 1 ? 0 : oz2);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const int ox = b == 0 ? ox0 : (b == 1 ? 0 : ox2);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
+        const int m3 = 3 * (n + oz + ox + oy);
+        const T* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
+        kv = fma(__ldg(s), __ldg(&u[m3]), kv);
+        kv = fma(__ldg(s + ndof), __ldg(&u[m3 + 1]), kv);
+        kv = fma(__ldg(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
+      }
+    }
+  }
+  return kv;
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T> p) {
   if (op_skip(p.io)) return;
   __shared__ double red[32];
   const Grid g = p.g;
-  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
-  const int NXY = NX * NY;
-  const int ndof = 3 * NXY * NZ;
-  const T* __restrict__ S = p.S;
+  const int ndof = 3 * (g.nx + 1) * (g.ny + 1) * (g.nz + 1);
   const T* __restrict__ u = p.io.u;
   double part = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ndof; i += gridDim.x * blockDim.x) {
     const int n = i / 3, c = i - 3 * n;
-    const int iy = n % NY, r = n / NY;
-    const int ix = r % NX, iz = r / NX;
-    const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
-    const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
-    const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
-    T kv = T(0);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const int oz = a == 0 ? oz0 : (a == 1 ? 0 : oz2);
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        const int ox = b == 0 ? ox0 : (b == 1 ? 0 : ox2);
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
-          const int m3 = 3 * (n + oz + ox + oy);
-          const T* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
-          kv = fma(__ldg(s), __ldg(&u[m3]), kv);
-          kv = fma(__ldg(s + ndof), __ldg(&u[m3 + 1]), kv);
-          kv = fma(__ldg(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
-        }
-      }
-    }
+    const T kv = stencil_row<T>(g, p.S, u, i);
     const bool fx = (p.fix[n] >> c) & 1;
     op_epilogue<T, MODE>(p.io, i, fx, kv, fx ? T(0) : u[i], epi_load<T, MODE>(p.io, i), part);
   }
@@ -301,14 +310,10 @@ inline dim3 plane_grid(int nxy, int nz) { return dim3((unsigned)((nxy + 255) / 2
 // neighbours are read unconditionally (offsets past the fine grid are clamped
 // and weighted 0), so the loads are independent.  Grid: plane_grid(CX*CY, CZ).
 template <typename T>
-__global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf,
-                                                       const uint8_t* __restrict__ fixc, T* bc, const int* done) {
-  if (done && *(volatile const int*)done) return;
+__device__ __forceinline__ void restrict_node(const Grid& gf, const Grid& gc, const T* __restrict__ rf,
+                                              const uint8_t* __restrict__ fixc, T* bc, int Ix, int Iy, int Iz) {
   const int FX = gf.nx + 1, FY = gf.ny + 1, FZ = gf.nz + 1;
   const int CX = gc.nx + 1, CY = gc.ny + 1;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= CX * CY) return;
-  const int Iz = blockIdx.y, Ix = t / CY, Iy = t - Ix * CY;
   const int FXY = FX * FY;
   T s0 = T(0), s1 = T(0), s2 = T(0);
 #pragma unroll
@@ -331,7 +336,7 @@ __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T
       }
     }
   }
-  const long long n = t + (long long)CX * CY * Iz;
+  const long long n = Iy + (long long)CY * (Ix + (long long)CX * Iz);
   const int f = fixc[n];
   T* dst = bc + 3 * n;
   dst[0] = (f & 1) ? T(0) : s0;
@@ -339,19 +344,26 @@ __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T
   dst[2] = (f & 4) ? T(0) : s2;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf,
+                                                       const uint8_t* __restrict__ fixc, T* bc, const int* done) {
+  if (done && *(volatile const int*)done) return;
+  const int CY = gc.ny + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (gc.nx + 1) * CY) return;
+  const int Ix = t / CY;
+  restrict_node<T>(gf, gc, rf, fixc, bc, Ix, t - Ix * CY, blockIdx.y);
+}
+
 // x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.  A fine node takes 1, 2, 4
 // or 8 coarse nodes (weights 1 or 1/2 per axis), read as a fixed 2x2x2 block
 // with zero weights for the absent ones.  Grid: plane_grid(FX*FY, FZ).
 template <typename T>
-__global__ void __launch_bounds__(256) prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc,
-                                                          const uint8_t* __restrict__ fixf, T* xf, const int* done) {
-  if (done && *(volatile const int*)done) return;
+__device__ __forceinline__ void prolong_node(const Grid& gf, const Grid& gc, const T* __restrict__ xc,
+                                             const uint8_t* __restrict__ fixf, T* xf, int ix, int iy, int iz) {
   const int FX = gf.nx + 1, FY = gf.ny + 1;
   const int CX = gc.nx + 1, CY = gc.ny + 1;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= FX * FY) return;
-  const int iz = blockIdx.y, ix = t / FY, iy = t - ix * FY;
-  const long long n = t + (long long)FX * FY * iz;
+  const long long n = iy + (long long)FY * (ix + (long long)FX * iz);
   const int f = fixf[n];
   if (f == 7) return;
   const int oy = iy & 1, ox = ix & 1, oz = iz & 1;
@@ -380,6 +392,17 @@ __global__ void __launch_bounds__(256) prolong_add_kernel(Grid gf, Grid gc, cons
   if (!(f & 1)) dst[0] += s0;
   if (!(f & 2)) dst[1] += s1;
   if (!(f & 4)) dst[2] += s2;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc,
+                                                          const uint8_t* __restrict__ fixf, T* xf, const int* done) {
+  if (done && *(volatile const int*)done) return;
+  const int FY = gf.ny + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (gf.nx + 1) * FY) return;
+  const int ix = t / FY;
+  prolong_node<T>(gf, gc, xc, fixf, xf, ix, t - ix * FY, blockIdx.y);
 }
 
 }  // namespace tp3d

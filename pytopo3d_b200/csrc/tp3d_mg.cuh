@@ -174,6 +174,128 @@ __global__ void __launch_bounds__(kBuildThreads) rap_kernel(Grid gf, Grid gc, co
         Ac[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
 }
 
+// ---- element-wise Galerkin products for levels >= 2 ----
+// With nested trilinear spaces every fine element maps into exactly one
+// coarse element of each level, so the level-L operator is the assembly of
+// level-L element matrices: for level 2, K2[C] = sum_f E_f Q_f^T KE Q_f over
+// the 4x4x4 fine elements f of C (tables KE2[f] = Q_f^T KE Q_f, f = fx + 4 fy +
+// 16 fz); for deeper levels K_L[C] = sum_s P_s^T K_{L-1}[C_s] P_s over the 8
+// sub-elements, P_s the trilinear interpolation to sub-element s.  Element
+// matrices are stored [element][24][24], element index as Grid::eidx.
+
+// Level-2 element matrices from the fine moduli; one block (576 threads, one
+// matrix entry each) per level-2 element.
+__global__ void __launch_bounds__(576) elem2_from_fine_kernel(Grid gf, Grid g2, const double* __restrict__ E,
+                                                              const double* __restrict__ KE2, double* K2) {
+  __shared__ double sE[64];
+  const int C = blockIdx.x;
+  const int cy = C % g2.ny, r = C / g2.ny;
+  const int cx = r % g2.nx, cz = r / g2.nx;
+  if (threadIdx.x < 64) {
+    const int x = 4 * cx + (threadIdx.x & 3), y = 4 * cy + ((threadIdx.x >> 2) & 3), z = 4 * cz + (threadIdx.x >> 4);
+    sE[threadIdx.x] = (x < gf.nx && y < gf.ny && z < gf.nz) ? __ldg(&E[gf.eidx(x, y, z)]) : 0.0;
+  }
+  __syncthreads();
+  double acc = 0.0;
+#pragma unroll 8
+  for (int f = 0; f < 64; ++f) acc = fma(sE[f], __ldg(&KE2[f * 576 + threadIdx.x]), acc);
+  K2[(size_t)C * 576 + threadIdx.x] = acc;
+}
+
+// Trilinear weight of coarse corner b at corner a of sub-element s.
+__device__ __forceinline__ double sub_weight(int s, int a, int b) {
+  const int px = corner_ox(s) + corner_ox(a) - 2 * corner_ox(b);
+  const int py = corner_oy(s) + corner_oy(a) - 2 * corner_oy(b);
+  const int pz = corner_oz(s) + corner_oz(a) - 2 * corner_oz(b);
+  return (px == 0 ? 1.0 : (px == 1 || px == -1 ? 0.5 : 0.0)) * (py == 0 ? 1.0 : (py == 1 || py == -1 ? 0.5 : 0.0)) *
+         (pz == 0 ? 1.0 : (pz == 1 || pz == -1 ? 0.5 : 0.0));
+}
+
+// Level-L element matrices from level L-1; one block (576 threads) per
+// level-L element.  Per sub-element: T = K_s (W_s x I3), then out += (W_s x I3)^T T.
+__global__ void __launch_bounds__(576) elem_coarsen_kernel(Grid gf, Grid gc, const double* __restrict__ Kf,
+                                                           double* Kc) {
+  __shared__ double sK[576], sT[576], sW[64];
+  const int C = blockIdx.x;
+  const int cy = C % gc.ny, r = C / gc.ny;
+  const int cx = r % gc.nx, cz = r / gc.nx;
+  const int t = threadIdx.x;
+  const int row = t / 24, col = t - 24 * row;  // output entry (row, col)
+  const int ra = row / 3, rc = row - 3 * ra, cb = col / 3, cd = col - 3 * cb;
+  double acc = 0.0;
+  for (int s = 0; s < 8; ++s) {
+    const int fx = 2 * cx + corner_ox(s), fy = 2 * cy + corner_oy(s), fz = 2 * cz + corner_oz(s);
+    if (fx >= gf.nx || fy >= gf.ny || fz >= gf.nz) continue;  // uniform over the block
+    __syncthreads();
+    sK[t] = __ldg(&Kf[(size_t)gf.eidx(fx, fy, fz) * 576 + t]);
+    if (t < 64) sW[t] = sub_weight(s, t >> 3, t & 7);  // sW[a * 8 + b]
+    __syncthreads();
+    // T[3a+c][3B+d] = sum_b' K_s[3a+c][3b'+d] W[b'][B]   (this thread: a = ra, c = rc, B = cb, d = cd)
+    double tv = 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) tv = fma(sK[row * 24 + 3 * b + cd], sW[b * 8 + cb], tv);
+    sT[t] = tv;
+    __syncthreads();
+    // out[3A+c][3B+d] += sum_a W[a][A] T[3a+c][3B+d]   (A = ra)
+#pragma unroll
+    for (int a = 0; a < 8; ++a) acc = fma(sW[a * 8 + ra], sT[(3 * a + rc) * 24 + col], acc);
+  }
+  Kc[(size_t)C * 576 + t] = acc;
+}
+
+// Stencil (27-point 3x3 blocks, layout of stencil_k) of level g assembled
+// from its element matrices.  Threads as in the other builders: a warp per 32
+// nodes for one (row component c, z-offset dzr).
+__global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid g, const double* __restrict__ Ke,
+                                                                           double* A) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = w / 3, dzr = w % 3 - 1;
+  const long long nn = g.nnode();
+  const long long n = (long long)blockIdx.x * 32 + lane;
+  if (n >= nn) return;
+  const int NY = g.ny + 1, NX = g.nx + 1;
+  const int iy = (int)(n % NY);
+  const long long r = n / NY;
+  const int ix = (int)(r % NX), iz = (int)(r / NX);
+  double acc[9][3];
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[i][d] = 0.0;
+#pragma unroll
+  for (int ez = -1; ez <= 0; ++ez) {
+    const int zc = iz + ez;
+    if (zc < 0 || zc >= g.nz) continue;
+#pragma unroll
+    for (int ex = -1; ex <= 0; ++ex) {
+      const int xc = ix + ex;
+      if (xc < 0 || xc >= g.nx) continue;
+#pragma unroll
+      for (int ey = -1; ey <= 0; ++ey) {
+        const int yc = iy + ey;
+        if (yc < 0 || yc >= g.ny) continue;
+        const int a = corner_index(-ex, -ey, -ez);
+        const double* rowp = Ke + (size_t)g.eidx(xc, yc, zc) * 576 + (3 * a + c) * 24;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          if (ez + corner_oz(b) != dzr) continue;
+          const int jx = ex + corner_ox(b), jy = ey + corner_oy(b);
+          const int slot = (jx + 1) * 3 + (jy + 1);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) acc[slot][d] += __ldg(&rowp[3 * b + d]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int jx = -1; jx <= 1; ++jx)
+#pragma unroll
+    for (int jy = -1; jy <= 1; ++jy)
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
+}
+
 // ---- coarse fixed-DOF masks ----
 // Injection: a coarse node takes the mask of the fine node it sits on (the
 // last fine node when it lies past an odd fine edge).  Dilation (fallback used
@@ -252,43 +374,40 @@ __global__ void dense_from_stencil_kernel(Grid g, const double* __restrict__ A, 
 // In-place Gauss-Jordan inverse of the SPD matrix D (n x n, row-major) into
 // Inv, one block, no pivoting (SPD pivots stay positive in exact arithmetic).
 // When `in_smem`, the matrix lives in dynamic shared memory (n <= 160).
+// Each pivot step copies row k and column k aside, then updates every entry
+// in one pass over the matrix, a warp per row (two barriers per step).
 // *status = 0 ok, k+1 if pivot k was not positive.
 __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const double* __restrict__ D, double* Inv,
                                                                 int in_smem, int* status) {
-  extern __shared__ double sA[];
-  double* A = in_smem ? sA : Inv;
-  __shared__ int bad;
-  __shared__ double piv;
+  extern __shared__ double sA[];  // [n * n if in_smem] [row k: n] [column k: n]
   const long long nn = (long long)n * n;
+  double* A = in_smem ? sA : Inv;
+  double* rowk = sA + (in_smem ? nn : 0);
+  double* colk = rowk + n;
+  __shared__ int bad;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   for (long long t = threadIdx.x; t < nn; t += blockDim.x) A[t] = D[t];
   if (threadIdx.x == 0) bad = 0;
   __syncthreads();
   for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) {
-      const double p = A[(size_t)k * n + k];
-      if (!(p > 0.0) && !bad) bad = k + 1;
-      piv = 1.0 / (p > 0.0 ? p : 1e-300);
-    }
-    __syncthreads();
-    const double pk = piv;
-    // entries off row k and column k, from the old row/column: a warp per row
-    for (int i = warp; i < n; i += nwarps) {
-      if (i == k) continue;
-      double* Ai = A + (size_t)i * n;
-      const double f = Ai[k] * pk;
-      const double* Ak = A + (size_t)k * n;
-      for (int j = lane; j < n; j += 32)
-        if (j != k) Ai[j] -= f * Ak[j];
-    }
-    __syncthreads();
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      if (t != k) {
-        A[(size_t)t * n + k] *= -pk;  // column k
-        A[(size_t)k * n + t] *= pk;   // row k
+      rowk[t] = A[(size_t)k * n + t];
+      colk[t] = A[(size_t)t * n + k];
+    }
+    __syncthreads();
+    const double p = rowk[k];
+    if (threadIdx.x == 0 && !(p > 0.0) && !bad) bad = k + 1;
+    const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
+    // a warp per row, lanes along the row
+    for (int i = warp; i < n; i += nwarps) {
+      double* Ai = A + (size_t)i * n;
+      const double f = colk[i] * pk;
+      if (i == k) {
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? pk : rowk[j] * pk;
+      } else {
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? -f : Ai[j] - f * rowk[j];
       }
     }
-    if (threadIdx.x == 0) A[(size_t)k * n + k] = pk;
     __syncthreads();
   }
   if (in_smem)

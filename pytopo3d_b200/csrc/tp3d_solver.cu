@@ -25,6 +25,7 @@
 
 #include "tp3d_fine.cuh"
 #include "tp3d_fine_wht.cuh"
+#include "tp3d_coarse.cuh"
 #include "tp3d_pcg.cuh"
 
 namespace tp3d {
@@ -188,6 +189,8 @@ struct tp3d_solver {
   bool ke_cls = false;              // KE has the cubic-symmetry class structure
   double kcls64[kKEClasses] = {};   // its class values
   double* KE1 = nullptr;
+  double* KE2 = nullptr;       // level-2 element tables (element-wise Galerkin)
+  std::vector<double*> Kel;    // element matrices of levels >= 2 (element-wise Galerkin)
   double penal = 3.0;
   bool have_density = false;
 
@@ -229,6 +232,11 @@ struct tp3d_solver {
   WhtTile wt64, wt32;
   bool use_wht64 = false, use_wht32 = false;
   bool fine_chosen = false;
+  // coarse end of the V-cycle as one cooperative launch from level cyc_L0
+  // (0: off); grid barrier state
+  int cyc_L0 = 0;
+  int cyc_blocks64 = 0, cyc_blocks32 = 0;
+  unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
 
   int last_iters = 0, last_updates = 0, last_restarts = 0;
@@ -362,7 +370,8 @@ struct tp3d_solver {
   }
   // Fine operator form for precision T: the dense-KE kernel or one of the
   // Walsh-Hadamard variants, whichever runs the Apply mode fastest on this
-  // grid (2 warm-up and 6 timed launches each, events on the solver stream);
+  // grid (2 warm-up launches, then the best of 3 rounds of 5, events on the
+  // solver stream);
   // fine_operator = 1 / 2 restricts the choice to one form.
   template <typename T>
   int choose_fine_form() {
@@ -389,14 +398,18 @@ struct tp3d_solver {
       io.out = out;
       for (int i = 0; i < 2; ++i)
         if (int rc = fine<T, kModeApply>(io)) return rc;
-      TP3D_CHECK(cudaEventRecord(a, st));
-      for (int i = 0; i < 6; ++i)
-        if (int rc = fine<T, kModeApply>(io)) return rc;
-      TP3D_CHECK(cudaEventRecord(b, st));
-      TP3D_CHECK(cudaEventSynchronize(b));
-      float f = 0.f;
-      TP3D_CHECK(cudaEventElapsedTime(&f, a, b));
-      *ms = f;
+      double best = 1e300;
+      for (int round = 0; round < 3; ++round) {
+        TP3D_CHECK(cudaEventRecord(a, st));
+        for (int i = 0; i < 5; ++i)
+          if (int rc = fine<T, kModeApply>(io)) return rc;
+        TP3D_CHECK(cudaEventRecord(b, st));
+        TP3D_CHECK(cudaEventSynchronize(b));
+        float f = 0.f;
+        TP3D_CHECK(cudaEventElapsedTime(&f, a, b));
+        best = std::min(best, (double)f);
+      }
+      *ms = best;
       return TP3D_OK;
     };
     double best = 1e300;
@@ -480,6 +493,65 @@ struct tp3d_solver {
     return rc;
   }
 
+  // Levels L .. nlev-1 of the V-cycle in one cooperative launch (rhs b on
+  // level L); returns the buffer holding level L's iterate.
+  template <typename T>
+  T* coarse_cycle(int L, const T* b, int* rc) {
+    auto& lvs = levels<T>();
+    CycleParams<T> p;
+    for (int k = L; k < nlev; ++k) {
+      CycleLevel<T>& c = p.lv[k];
+      c.g = grids[k];
+      c.S = lvs[k].A;
+      c.fix = fix[k];
+      c.dinv = lvs[k].dinv;
+      c.coef = coef[k];
+      c.x[0] = lvs[k].x[0];
+      c.x[1] = lvs[k].x[1];
+      c.b = lvs[k].b;
+      c.r = lvs[k].r;
+      c.d = lvs[k].d;
+    }
+    p.lv[L].b = const_cast<T*>(b);
+    p.L0 = L;
+    p.Lc = nlev - 1;
+    p.pre = o.pre_sweeps;
+    p.post = o.post_sweeps;
+    p.cheb = o.smoother != 1 ? 1 : 0;
+    p.omega = (T)o.omega;
+    p.cn = cn;
+    if constexpr (sizeof(T) == 8) p.inv = cinv64;
+    else p.inv = cinv32;
+    p.done = &state->done;
+    p.bar = cyc_bar;
+    p.bar_err = (int*)(cyc_bar + 1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(sizeof(T) == 8 ? cyc_blocks64 : cyc_blocks32));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, coarse_cycle_kernel<T>, p) != cudaSuccess) *rc = TP3D_ERR_CUDA;
+    count_launch();
+    return L == nlev - 1 ? lvs[L].x[0] : lvs[L].x[cycle_final_buffer(o.pre_sweeps, o.post_sweeps)];
+  }
+
+  // Cooperative grid for the coarse cycle from level L: enough blocks for
+  // one DOF per thread on level L, at most what can be co-resident.
+  template <typename T>
+  int cycle_blocks(int L) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, coarse_cycle_kernel<T>, 256, 0) != cudaSuccess ||
+        occ < 1)
+      return 0;
+    const long long need = (3 * grids[L].nnode() + 255) / 256;
+    return (int)std::max<long long>(1, std::min<long long>(need, (long long)occ * nsm));
+  }
+
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
   T* vcycle(int L, const T* b, const int* done, int* rc) {
@@ -500,6 +572,7 @@ struct tp3d_solver {
       count_launch();
       return lv.x[0];
     }
+    if (L == cyc_L0 && cyc_L0 > 0) return coarse_cycle<T>(L, b, rc);
     const bool cheb = o.smoother != 1;
     int cur = 0;
     smooth_zero_kernel<T><<<grid_blocks(ndof), 256, 0, st>>>(ndof, b, lv.dinv, (T)o.omega, cheb ? coef[L] : nullptr,
@@ -595,6 +668,10 @@ struct tp3d_solver {
     if (s.done == 3 || s.done == 4) {
       tp3d_set_last_error(s.done == 3 ? "CG breakdown (p'Ap <= 0)" : "non-finite residual in CG");
       return TP3D_ERR_NONFINITE;
+    }
+    if (s.done == 7) {
+      tp3d_set_last_error("coarse-cycle grid barrier expired");
+      return TP3D_ERR_TIMEOUT;
     }
     return TP3D_NOT_CONVERGED;
   }
@@ -794,7 +871,7 @@ struct tp3d_solver {
     last_updates = s.updates;
     last_relres = s.bb > 0.0 ? std::sqrt(std::max(s.rr_hi, 0.0) / s.bb) : 0.0;
     last_fallback = false;
-    if (s.done == 1 || s.done == 5) return status_of(s);
+    if (s.done == 1 || s.done == 5 || s.done == 7) return status_of(s);
     // FP32 could not resolve this system (cap, breakdown, non-finite, or a
     // stall far above the target): finish it with the FP64 solver.
     if (int e = ensure_fp64_buffers()) return e;
@@ -873,6 +950,33 @@ static void coarse_subelement_tables(const double* KE, double* out) {
   }
 }
 
+// KE2[f] = Q_f^T KE Q_f for the 64 fine elements f = fx + 4 fy + 16 fz of a
+// level-2 element: Q_f interpolates from the level-2 element's corners to
+// fine element f's corners, weights prod(1 - |pos - 4 o(b)| / 4), pos = f + o(a).
+static void level2_element_tables(const double* KE, double* out) {
+  for (int f = 0; f < 64; ++f) {
+    const int fx = f & 3, fy = (f >> 2) & 3, fz = f >> 4;
+    double W[8][8];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b)
+        W[a][b] = std::max(0.0, 1.0 - std::abs(fx + corner_ox(a) - 4 * corner_ox(b)) / 4.0) *
+                  std::max(0.0, 1.0 - std::abs(fy + corner_oy(a) - 4 * corner_oy(b)) / 4.0) *
+                  std::max(0.0, 1.0 - std::abs(fz + corner_oz(a) - 4 * corner_oz(b)) / 4.0);
+    for (int A = 0; A < 8; ++A)
+      for (int c = 0; c < 3; ++c)
+        for (int B = 0; B < 8; ++B)
+          for (int d = 0; d < 3; ++d) {
+            double t = 0.0;
+            for (int a = 0; a < 8; ++a) {
+              if (W[a][A] == 0.0) continue;
+              for (int b = 0; b < 8; ++b)
+                if (W[b][B] != 0.0) t += W[a][A] * KE[(3 * a + c) * 24 + 3 * b + d] * W[b][B];
+            }
+            out[(size_t)f * 576 + (3 * A + c) * 24 + 3 * B + d] = t;
+          }
+  }
+}
+
 extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   if (!o) return;
   o->precision = TP3D_PRECISION_FP64;
@@ -890,6 +994,8 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->reliable_delta = 0.05;
   o->max_restarts = 3;
   o->fine_operator = 0;
+  o->fused_cycle_dofs = 0;
+  o->galerkin = 0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -954,7 +1060,22 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   }
   if (3 * s->grids.back().nnode() > 3000) s->grids.resize(1);  // dense coarsest would be too large
   s->nlev = (int)s->grids.size();
+  // first level (>= 1, above the coarsest) small enough for the fused coarse cycle
+  s->cyc_L0 = 0;
+  if (o.fused_cycle_dofs > 0)
+    for (int L = 1; L < s->nlev - 1; ++L)
+      if (3 * s->grids[L].nnode() <= o.fused_cycle_dofs) {
+        s->cyc_L0 = L;
+        break;
+      }
+  if (s->nlev > kCycleMaxLevels) s->cyc_L0 = 0;
 
+  if (s->cyc_L0 > 0) {
+    s->cyc_blocks64 = s->cycle_blocks<double>(s->cyc_L0);
+    s->cyc_blocks32 = s->cycle_blocks<float>(s->cyc_L0);
+    s->cyc_bar = s->alloc<unsigned int>(2);
+    if (!s->cyc_blocks64 || !s->cyc_blocks32 || !s->cyc_bar) s->cyc_L0 = 0;
+  }
   s->partials = s->alloc<double>(kMaxPartials);
   s->state = s->alloc<PcgState>(1);
   unsigned int* cnt = s->alloc<unsigned int>(4);
@@ -986,6 +1107,15 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   coarse_subelement_tables(KE_host, ke1);
   s->KE1 = s->alloc<double>(8 * 576);
   cudaMemcpy(s->KE1, ke1, sizeof(ke1), cudaMemcpyHostToDevice);
+  if (o.galerkin < 0 || o.galerkin > 1) return fail(TP3D_ERR_ARG, "invalid galerkin option");
+  if (o.galerkin == 0 && s->nlev > 2) {
+    std::vector<double> ke2((size_t)64 * 576);
+    level2_element_tables(KE_host, ke2.data());
+    s->KE2 = s->alloc<double>(64 * 576);
+    if (s->KE2) cudaMemcpy(s->KE2, ke2.data(), ke2.size() * sizeof(double), cudaMemcpyHostToDevice);
+    s->Kel.assign(s->nlev, nullptr);
+    for (int L = 2; L < s->nlev; ++L) s->Kel[L] = s->alloc<double>((size_t)576 * s->grids[L].nele());
+  }
   s->A64.assign(s->nlev, nullptr);
   s->L64.resize(s->nlev);
   if (mixed) s->L32.resize(s->nlev);
@@ -1136,6 +1266,12 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     const unsigned nb = (unsigned)((gc.nnode() + 31) / 32);
     if (L == 1) {
       build_level1_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1]);
+    } else if (s->o.galerkin == 0) {
+      const unsigned ne = (unsigned)gc.nele();
+      if (L == 2) elem2_from_fine_kernel<<<ne, 576, 0, st>>>(s->grids[0], gc, s->E64, s->KE2, s->Kel[2]);
+      else elem_coarsen_kernel<<<ne, 576, 0, st>>>(gf, gc, s->Kel[L - 1], s->Kel[L]);
+      count_launch();
+      stencil_from_elems_kernel<<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L]);
     } else {
       rap_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->A64[L - 1], s->A64[L]);
     }
@@ -1168,7 +1304,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       }
       {
         const int in_smem = n <= 160 ? 1 : 0;
-        const size_t smem = in_smem ? (size_t)n * n * sizeof(double) : 0;
+        const size_t smem = ((in_smem ? (size_t)n * n : 0) + 2 * (size_t)n) * sizeof(double);
         if (smem > 48 * 1024)
           TP3D_CHECK(cudaFuncSetAttribute(dense_gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
@@ -1220,6 +1356,7 @@ extern "C" int tp3d_solver_solve(tp3d_solver* s, const double* F, double* U, int
   cudaStream_t st = s->st;
   const long long nn = s->g.nnode(), ndof = 3 * nn;
   if (int e = s->enter()) return e;
+  if (s->cyc_bar) TP3D_CHECK(cudaMemsetAsync(s->cyc_bar, 0, 2 * sizeof(unsigned int), st));
   TP3D_CHECK(cudaMemcpyAsync(s->u64, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
   zero_fixed_kernel<<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->u64, s->fix[0]); count_launch();
   s->last_updates = 0;
@@ -1308,7 +1445,8 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)s->tile.ZC, s->coarse_fallback ? 1.0 : 0.0, lam.empty() ? 0.0 : lam[0],
                            s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0,
                            s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
-                           s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0};
+                           s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0,
+                           (double)s->cyc_L0};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;
