@@ -405,10 +405,17 @@ def run_probe(args):
         for _ in range(max(1, args.warmup)):
             loop.step()
         torch.cuda.synchronize()
+        oc_steps, cg = [], 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         for _ in range(args.steps):
-            loop.step()
+            oc_steps.append(loop.step()[3:4])
+            cg += loop.last["cg_iterations"]
+        e1.record()
         torch.cuda.synchronize()
         print(json.dumps({"mode": "step", "size": [NELX, NELY, NELZ], "steps": args.steps,
+                          "ms_per_step": e0.elapsed_time(e1) / args.steps, "cg_per_step": cg / args.steps,
+                          "options": opts, "bisection_steps": [float(t.item()) for t in oc_steps],
                           "solver": loop.solver.stats()}))
     else:
         # moduli + hierarchy only (no solve), so the first launches of the

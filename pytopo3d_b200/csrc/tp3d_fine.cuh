@@ -60,6 +60,7 @@ __device__ __forceinline__ EpiIn<T> fine_epi_load(int mode, const OpIO<T>& io, l
     case kModeChebFirst: return epi_load<T, kModeChebFirst>(io, i);
     case kModeChebStep: return epi_load<T, kModeChebStep>(io, i);
     case kModeDinvApply: return epi_load<T, kModeDinvApply>(io, i);
+    case kModeChebStepDot: return epi_load<T, kModeChebStepDot>(io, i);
     default: return EpiIn<T>{};
   }
 }
@@ -74,6 +75,7 @@ __device__ __forceinline__ void fine_epilogue(int mode, const OpIO<T>& io, long 
     case kModeCgQ: op_epilogue<T, kModeCgQ>(io, i, fx, kv, own, in, part); break;
     case kModeChebFirst: op_epilogue<T, kModeChebFirst>(io, i, fx, kv, own, in, part); break;
     case kModeChebStep: op_epilogue<T, kModeChebStep>(io, i, fx, kv, own, in, part); break;
+    case kModeChebStepDot: op_epilogue<T, kModeChebStepDot>(io, i, fx, kv, own, in, part); break;
     default: op_epilogue<T, kModeDinvApply>(io, i, fx, kv, own, in, part); break;
   }
 }
@@ -279,9 +281,11 @@ __global__ void __launch_bounds__(256, 2) fine_apply_kernel(const __grid_constan
     }
     __syncthreads();
   }
-  if (p.mode == kModeCgQ) {
+  if (p.mode == kModeCgQ || p.mode == kModeChebStepDot) {
     part = block_sum(part, red);
     if (tid == 0) p.io.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
+    if (p.io.fin_count)
+      last_block_finalize(p.io.partials, gridDim.x * gridDim.y, p.io.fin_count, p.io.fin, p.io.fin_op, red);
   }
 }
 

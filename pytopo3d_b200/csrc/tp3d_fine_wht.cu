@@ -40,6 +40,7 @@ struct WhtVariant {
       case kModeCgQ: return fn<kModeCgQ>();
       case kModeChebFirst: return fn<kModeChebFirst>();
       case kModeChebStep: return fn<kModeChebStep>();
+      case kModeChebStepDot: return fn<kModeChebStepDot>();
       default: return fn<kModeDinvApply>();
     }
   }
@@ -61,7 +62,7 @@ bool wht_prepare(int v) {
   if (done[v]) return true;
   const int nthr = WhtShapes<T>::nthr[v];
   const int smem = (int)wht_smem_bytes<T>(nthr);
-  for (int mode = 0; mode <= kModeDinvApply; ++mode)
+  for (int mode = 0; mode <= kModeChebStepDot; ++mode)
     if (cudaFuncSetAttribute(wht_fn<T, ESrc>(mode, v), cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
         cudaSuccess)
       return false;

@@ -233,9 +233,11 @@ __global__ void __launch_bounds__(NTHR, MINB) wht_apply_kernel(const __grid_cons
     }
     En = En2;
   }
-  if constexpr (MODE == kModeCgQ) {
+  if constexpr (mode_reduces<MODE>()) {
     part = block_sum(part, red);
     if (t == 0) p.io.partials[blockIdx.y * gridDim.x + blockIdx.x] = part;
+    if (p.io.fin_count)
+      last_block_finalize(p.io.partials, gridDim.x * gridDim.y, p.io.fin_count, p.io.fin, p.io.fin_op, red);
   }
 }
 

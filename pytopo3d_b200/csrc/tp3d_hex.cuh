@@ -16,6 +16,7 @@
 // with the coarse fixed DOFs masked out for the apply kernels.
 #pragma once
 
+#include "tp3d_cgstate.cuh"
 #include "tp3d_common.cuh"
 
 namespace tp3d {
@@ -55,6 +56,7 @@ enum ApplyMode : int {
   kModeChebFirst = 4,  // d = c0 Dinv (b - K u); out = u + d
   kModeChebStep = 5,   // d = c1 d + c2 Dinv (b - K u); out = u + d
   kModeDinvApply = 6,  // out = Dinv K u (power iteration for lambda_max(Dinv K))
+  kModeChebStepDot = 7,  // as kModeChebStep, and partials += b . out (the CG's r . z)
 };
 
 // Inputs / outputs shared by every operator kernel.
@@ -71,6 +73,11 @@ struct OpIO {
   double* partials = nullptr;
   const int* done = nullptr;  // skip when *done != 0
   const int* gate = nullptr;  // skip when *gate == 0
+  // reductions (kModeCgQ, kModeChebStepDot): when fin_count is set, the last
+  // block finishes the reduction and applies finalize op fin_op to *fin
+  PcgState* fin = nullptr;
+  int fin_op = 0;
+  unsigned int* fin_count = nullptr;
 };
 
 template <typename T>
@@ -87,11 +94,17 @@ struct EpiIn {
 
 template <int MODE>
 __host__ __device__ constexpr bool epi_reads_b() {
-  return MODE == kModeResid || MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep;
+  return MODE == kModeResid || MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep ||
+         MODE == kModeChebStepDot;
 }
 template <int MODE>
 __host__ __device__ constexpr bool epi_reads_dinv() {
-  return MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep || MODE == kModeDinvApply;
+  return MODE == kModeJacobi || MODE == kModeChebFirst || MODE == kModeChebStep || MODE == kModeDinvApply ||
+         MODE == kModeChebStepDot;
+}
+template <int MODE>
+__host__ __device__ constexpr bool mode_reduces() {
+  return MODE == kModeCgQ || MODE == kModeChebStepDot;
 }
 
 template <typename T, int MODE>
@@ -99,7 +112,7 @@ __device__ __forceinline__ EpiIn<T> epi_load(const OpIO<T>& io, long long i) {
   EpiIn<T> in;
   if (epi_reads_b<MODE>()) in.b = io.b[i];
   if (epi_reads_dinv<MODE>()) in.dinv = io.dinv[i];
-  if (MODE == kModeChebStep) in.d = io.d[i];
+  if (MODE == kModeChebStep || MODE == kModeChebStepDot) in.d = io.d[i];
   return in;
 }
 
@@ -121,10 +134,12 @@ __device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool
     const T dd = fx ? T(0) : (T)io.coef[0] * in.dinv * (in.b - kv);
     io.d[i] = dd;
     io.out[i] = own + dd;
-  } else if (MODE == kModeChebStep) {
+  } else if (MODE == kModeChebStep || MODE == kModeChebStepDot) {
     const T dd = fx ? T(0) : (T)io.coef[2 * io.step] * in.d + (T)io.coef[2 * io.step + 1] * in.dinv * (in.b - kv);
     io.d[i] = dd;
-    io.out[i] = own + dd;
+    const T z = own + dd;
+    io.out[i] = z;
+    if (MODE == kModeChebStepDot) part += (double)in.b * (double)z;
   } else {  // kModeDinvApply
     io.out[i] = fx ? T(0) : in.dinv * kv;
   }
@@ -260,9 +275,10 @@ __global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constan
     const bool fx = (p.fix[n] >> c) & 1;
     op_epilogue<T, MODE>(p.io, i, fx, kv, fx ? T(0) : u[i], epi_load<T, MODE>(p.io, i), part);
   }
-  if (MODE == kModeCgQ) {
+  if (mode_reduces<MODE>()) {
     part = block_sum(part, red);
     if (threadIdx.x == 0) p.io.partials[blockIdx.x] = part;
+    if (p.io.fin_count) last_block_finalize(p.io.partials, gridDim.x, p.io.fin_count, p.io.fin, p.io.fin_op, red);
   }
 }
 
@@ -344,15 +360,39 @@ __device__ __forceinline__ void restrict_node(const Grid& gf, const Grid& gc, co
   dst[2] = (f & 4) ? T(0) : s2;
 }
 
+// First smoothing step of the coarse level from a zero guess, fused into the
+// restriction (it is pointwise): x0 = w dinv b with w = omega or (coef given)
+// the Chebyshev c0, and d = x0 when d is given.  x0 == nullptr: none.
+template <typename T>
+struct CoarseFirstStep {
+  const T* dinv = nullptr;
+  const double* coef = nullptr;
+  T omega = T(0);
+  T* x0 = nullptr;
+  T* d = nullptr;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf,
-                                                       const uint8_t* __restrict__ fixc, T* bc, const int* done) {
+                                                       const uint8_t* __restrict__ fixc, T* bc, const int* done,
+                                                       CoarseFirstStep<T> fs) {
   if (done && *(volatile const int*)done) return;
   const int CY = gc.ny + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (gc.nx + 1) * CY) return;
-  const int Ix = t / CY;
-  restrict_node<T>(gf, gc, rf, fixc, bc, Ix, t - Ix * CY, blockIdx.y);
+  const int Ix = t / CY, Iy = t - Ix * CY;
+  restrict_node<T>(gf, gc, rf, fixc, bc, Ix, Iy, blockIdx.y);
+  if (fs.x0) {
+    const T w = fs.coef ? (T)fs.coef[0] : fs.omega;
+    const long long n = Iy + (long long)CY * (Ix + (long long)(gc.nx + 1) * blockIdx.y);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      const T v = w * fs.dinv[i] * bc[i];
+      fs.x0[i] = v;
+      if (fs.d) fs.d[i] = v;
+    }
+  }
 }
 
 // x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.  A fine node takes 1, 2, 4

@@ -4,150 +4,27 @@
 // captured into a CUDA graph and replayed without host round trips.
 #pragma once
 
+#include "tp3d_cgstate.cuh"
 #include "tp3d_mg.cuh"
 
 namespace tp3d {
 
-struct PcgState {
-  double rz, pq, rr, bb, alpha, beta, tol2, rmax2;
-  double delta2;   // reliable-update threshold (squared)
-  double rr_hi;    // last FP64 residual norm^2
-  double rr_best;  // smallest FP64 residual norm^2 so far
-  // done: 0 running, 1 converged, 2 iteration cap, 3 breakdown, 4 non-finite,
-  //       5 FP64 residual stalled at its attainable floor (accepted),
-  //       6 FP64 residual stalled far above the target (mixed: fall back to FP64)
-  int done;
-  int iters, max_iters;
-  int update;   // mixed precision: replace the residual this iteration
-  int updates;  // count of reliable updates
-  int stall;    // consecutive reliable updates that did not halve the FP64 residual
-  int restart;  // mixed precision: FP32 p'Ap <= 0, restart the direction from z
-  int nbreak;   // consecutive restarts
-};
-
-enum FinalizeOp : int {
-  kFinBB = 0,    // bb = ||b||^2, tol2 = rtol^2 bb
-  kFinRRInit,    // rr = ||r0||^2 (stop if already converged)
-  kFinRZInit,    // rz = r.z
-  kFinPQ,        // alpha = rz / p.q
-  kFinRR,        // rr = ||r||^2, iteration count, stop test
-  kFinRZ,        // beta = rz_new / rz
-  kFinRRMixed,   // FP32 recursive residual: decide on a reliable update
-  kFinRRHi,      // FP64 true residual after a reliable update: stop test
-  kFinValue,     // plain sum into *out (no state change)
-  kFinPQMixed,   // as kFinPQ, but a non-positive FP32 p'Ap restarts the direction
-  kFinRZMixed,   // as kFinRZ, honouring a pending restart (beta = 0)
-};
-
 __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgState* st, int op, double rtol2,
                                 double* out) {
   __shared__ double red[32];
-  if (((op >= kFinPQ && op <= kFinRRMixed) || op >= kFinPQMixed) && *(volatile int*)&st->done) return;
-  if (op == kFinRRHi && (*(volatile int*)&st->done || *(volatile int*)&st->update == 0)) return;
+  if (finalize_skipped(st, op)) return;
   const double s = sum_partials(partials, n, red);
   if (threadIdx.x != 0) return;
-  switch (op) {
-    case kFinBB:
-      st->bb = s;
-      st->tol2 = rtol2 * s;
-      st->iters = 0;
-      st->update = 0;
-      st->updates = 0;
-      st->done = (s == 0.0) ? 1 : 0;
-      if (!isfinite(s)) st->done = 4;
-      break;
-    case kFinRRInit:
-      st->rr = s;
-      st->rmax2 = s;
-      st->rr_hi = s;
-      st->rr_best = s;
-      st->stall = 0;
-      if (!st->done && s <= st->tol2) st->done = 1;
-      if (!isfinite(s)) st->done = 4;
-      break;
-    case kFinRZInit:
-      st->rz = s;
-      break;
-    case kFinPQ:
-      st->pq = s;
-      if (!(s > 0.0) || !isfinite(s)) st->done = 3;
-      else st->alpha = st->rz / s;
-      break;
-    case kFinRR:
-      st->rr = s;
-      st->iters += 1;
-      if (!isfinite(s)) st->done = 4;
-      else if (s <= st->tol2) st->done = 1;
-      else if (st->iters >= st->max_iters) st->done = 2;
-      break;
-    case kFinRZ:
-      st->beta = s / st->rz;
-      st->rz = s;
-      break;
-    case kFinRRMixed:
-      st->rr = s;
-      st->iters += 1;
-      if (!isfinite(s)) {
-        st->done = 4;
-      } else {
-        st->update = (st->restart || s <= st->delta2 * st->rmax2 || s <= st->tol2 || st->iters >= st->max_iters)
-                         ? 1
-                         : 0;
-      }
-      break;
-    case kFinRRHi:
-      st->rr_hi = s;
-      st->rmax2 = s;
-      st->updates += 1;
-      if (!isfinite(s)) {
-        st->done = 4;
-      } else if (s <= st->tol2) {
-        st->done = 1;
-      } else {
-        st->stall = (s > 0.25 * st->rr_best) ? st->stall + 1 : 0;
-        st->rr_best = fmin(st->rr_best, s);
-        // a stall is an attainable floor only once the residual is small; a stall
-        // above 1e-6 relative is a failure (the host then falls back to FP64)
-        if (st->stall >= 3) st->done = (s <= 1e-12 * st->bb) ? 5 : 6;
-        else if (st->iters >= st->max_iters) st->done = 2;
-      }
-      break;
-    case kFinValue:
-      *out = s;
-      break;
-    case kFinPQMixed:
-      // FP32 rounding next to 1e-9 voids can make p'Ap non-positive although K
-      // is SPD: skip the step (alpha = 0), force a reliable update and restart
-      // the direction from the new preconditioned residual.
-      st->pq = s;
-      if (!isfinite(s)) {
-        st->done = 4;
-      } else if (!(s > 0.0)) {
-        st->alpha = 0.0;
-        st->restart = 1;
-        if (++st->nbreak > 5) st->done = 3;
-      } else {
-        st->alpha = st->rz / s;
-      }
-      break;
-    case kFinRZMixed:
-      if (st->restart) {
-        st->beta = 0.0;
-        st->restart = 0;
-      } else {
-        st->beta = s / st->rz;
-        st->nbreak = 0;
-      }
-      st->rz = s;
-      break;
-  }
+  finalize_apply(s, st, op, rtol2, out);
 }
 
 __global__ void clear_update_kernel(PcgState* st) { st->update = 0; }
 
+// a . b into per-block partials; with fin_count, the last block applies op to st.
 template <typename T>
 __global__ void dot_kernel(long long n, const T* __restrict__ a, const T* __restrict__ b, double* partials,
-                           const int* done, const int* gate) {
+                           const int* done, const int* gate, PcgState* st = nullptr, int op = 0,
+                           unsigned int* fin_count = nullptr) {
   if ((done && *(volatile const int*)done) || (gate && *(volatile const int*)gate == 0)) return;
   __shared__ double red[32];
   double s = 0.0;
@@ -155,6 +32,7 @@ __global__ void dot_kernel(long long n, const T* __restrict__ a, const T* __rest
     s += (double)a[i] * (double)b[i];
   s = block_sum(s, red);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (fin_count) last_block_finalize(partials, gridDim.x, fin_count, st, op, red);
 }
 
 // ||b||^2 over free DOFs
@@ -172,10 +50,11 @@ __global__ void masked_norm_kernel(long long nn, const double* __restrict__ b, c
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-// u += alpha p; r -= alpha q; partials of ||r||^2
+// u += alpha p; r -= alpha q; partials of ||r||^2 (with fin_count, the last
+// block applies op to st)
 template <typename T>
 __global__ void cg_update_kernel(long long n, T* u, const T* __restrict__ p, T* r, const T* __restrict__ q,
-                                 const PcgState* st, double* partials) {
+                                 PcgState* st, double* partials, int op = 0, unsigned int* fin_count = nullptr) {
   if (*(volatile const int*)&st->done) return;
   __shared__ double red[32];
   const T a = (T)st->alpha;
@@ -188,6 +67,7 @@ __global__ void cg_update_kernel(long long n, T* u, const T* __restrict__ p, T* 
   }
   s = block_sum(s, red);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  if (fin_count) last_block_finalize(partials, gridDim.x, fin_count, st, op, red);
 }
 
 // p = z + beta p (or p = z)

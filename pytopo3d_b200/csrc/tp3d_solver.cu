@@ -221,6 +221,7 @@ struct tp3d_solver {
   double* F_capture = nullptr;  // the mixed graph reads F from here
 
   double* partials = nullptr;
+  unsigned int* fin_count = nullptr;  // arrivals of the reduction in flight (last_block_finalize)
   PcgState* state = nullptr;
   PcgState* state_host = nullptr;  // two pinned slots
   Tile tile;
@@ -445,14 +446,6 @@ struct tp3d_solver {
     return TP3D_OK;
   }
 
-  template <typename T>
-  int fine_partials() const {
-    if (use_wht<T>()) {
-      const WhtTile& w = wtile<T>();
-      return w.tiles_y * w.tiles_x * w.zchunks;
-    }
-    return tile.tiles_y * tile.tiles_x * tile.zchunks;
-  }
 
 
   template <typename T, int MODE>
@@ -471,7 +464,9 @@ struct tp3d_solver {
 
   // ---------------- V-cycle ----------------
   template <typename T>
-  int smooth_steps(int L, int first_step, int nsteps, int* cur, const T* b, const int* done) {
+  // dot_op >= 0: the last step is a Chebyshev step (s >= 1) that also reduces
+  // b . out and applies finalize op dot_op (the caller checked it applies).
+  int smooth_steps(int L, int first_step, int nsteps, int* cur, const T* b, const int* done, int dot_op = -1) {
     auto& lv = levels<T>()[L];
     int rc = TP3D_OK;
     for (int s = first_step; s < first_step + nsteps; ++s) {
@@ -485,9 +480,19 @@ struct tp3d_solver {
       io.step = s;
       io.omega = (T)o.omega;
       io.done = done;
-      if (o.smoother == 1) rc |= apply_level<T, kModeJacobi>(L, io);
-      else if (s == 0) rc |= apply_level<T, kModeChebFirst>(L, io);
-      else rc |= apply_level<T, kModeChebStep>(L, io);
+      if (dot_op >= 0 && s == first_step + nsteps - 1) {
+        io.partials = partials;
+        io.fin = state;
+        io.fin_op = dot_op;
+        io.fin_count = fin_count;
+        rc |= apply_level<T, kModeChebStepDot>(L, io);
+      } else if (o.smoother == 1) {
+        rc |= apply_level<T, kModeJacobi>(L, io);
+      } else if (s == 0) {
+        rc |= apply_level<T, kModeChebFirst>(L, io);
+      } else {
+        rc |= apply_level<T, kModeChebStep>(L, io);
+      }
       *cur = 1 - *cur;
     }
     return rc;
@@ -554,7 +559,14 @@ struct tp3d_solver {
 
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
-  T* vcycle(int L, const T* b, const int* done, int* rc) {
+  // zero_done: the first smoothing step from zero already ran (fused into the
+  // restriction that produced b).
+  // dot_op >= 0 (level 0 only): when the last post-smoothing step is a
+  // Chebyshev step, it also reduces b . x and applies finalize op dot_op;
+  // *dot_done tells the caller whether it did.
+  T* vcycle(int L, const T* b, const int* done, int* rc, bool zero_done = false, int dot_op = -1,
+            bool* dot_done = nullptr) {
+    if (dot_done) *dot_done = false;
     auto& lv = levels<T>()[L];
     const Grid& gl = grids[L];
     const long long ndof = 3 * gl.nnode();
@@ -575,9 +587,11 @@ struct tp3d_solver {
     if (L == cyc_L0 && cyc_L0 > 0) return coarse_cycle<T>(L, b, rc);
     const bool cheb = o.smoother != 1;
     int cur = 0;
-    smooth_zero_kernel<T><<<grid_blocks(ndof), 256, 0, st>>>(ndof, b, lv.dinv, (T)o.omega, cheb ? coef[L] : nullptr,
-                                                             lv.x[cur], cheb ? lv.d : nullptr, done);
-    count_launch();
+    if (!zero_done) {
+      smooth_zero_kernel<T><<<grid_blocks(ndof), 256, 0, st>>>(ndof, b, lv.dinv, (T)o.omega, cheb ? coef[L] : nullptr,
+                                                               lv.x[cur], cheb ? lv.d : nullptr, done);
+      count_launch();
+    }
     *rc |= smooth_steps<T>(L, 1, o.pre_sweeps - 1, &cur, b, done);
     {
       OpIO<T> io;
@@ -589,14 +603,26 @@ struct tp3d_solver {
     }
     auto& lc = levels<T>()[L + 1];
     const Grid& gn = grids[L + 1];
+    // the next level's first smoothing step rides along when that level smooths
+    const bool fuse_first = L + 1 < nlev - 1 && !(L + 1 == cyc_L0 && cyc_L0 > 0);
+    CoarseFirstStep<T> fs;
+    if (fuse_first) {
+      fs.dinv = lc.dinv;
+      fs.coef = cheb ? coef[L + 1] : nullptr;
+      fs.omega = (T)o.omega;
+      fs.x0 = lc.x[0];
+      fs.d = cheb ? lc.d : nullptr;
+    }
     restrict_kernel<T><<<plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), 256, 0, st>>>(gl, gn, lv.r, fix[L + 1], lc.b,
-                                                                           done);
+                                                                           done, fs);
     count_launch();
-    T* xc = vcycle<T>(L + 1, lc.b, done, rc);
+    T* xc = vcycle<T>(L + 1, lc.b, done, rc, fuse_first);
     prolong_add_kernel<T><<<plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1), 256, 0, st>>>(gl, gn, xc, fix[L],
                                                                                              lv.x[cur], done);
     count_launch();
-    *rc |= smooth_steps<T>(L, 0, o.post_sweeps, &cur, b, done);
+    const bool dot_here = dot_op >= 0 && o.smoother != 1 && o.post_sweeps >= 2;
+    *rc |= smooth_steps<T>(L, 0, o.post_sweeps, &cur, b, done, dot_here ? dot_op : -1);
+    if (dot_here && dot_done) *dot_done = true;
     if (cudaGetLastError() != cudaSuccess) *rc = TP3D_ERR_CUDA;
     return lv.x[cur];
   }
@@ -687,13 +713,18 @@ struct tp3d_solver {
     io.out = K.q;
     io.partials = partials;
     io.done = done;
+    io.fin = state;
+    io.fin_op = kFinPQ;
+    io.fin_count = fin_count;
     int rc = fine<double, kModeCgQ>(io);
-    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials<double>(), state, kFinPQ, 0.0, nullptr); count_launch();
-    cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRR, 0.0, nullptr); count_launch();
-    double* z = vcycle<double>(0, K.r, done, &rc);
-    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZ, 0.0, nullptr); count_launch();
+    cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRR, fin_count);
+    count_launch();
+    bool dot_done = false;
+    double* z = vcycle<double>(0, K.r, done, &rc, false, kFinRZ, &dot_done);
+    if (!dot_done) {
+      dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZ, fin_count);
+      count_launch();
+    }
     cg_p_kernel<double><<<nb, 256, 0, st>>>(ndof, z, K.p, state, 0); count_launch();
     TP3D_CHECK_LAUNCH();
     return rc;
@@ -804,11 +835,12 @@ struct tp3d_solver {
     io.out = K.q;
     io.partials = partials;
     io.done = done;
+    io.fin = state;
+    io.fin_op = kFinPQMixed;
+    io.fin_count = fin_count;
     int rc = fine<float, kModeCgQ>(io);
-    finalize_kernel<<<1, 256, 0, st>>>(partials, fine_partials<float>(), state, kFinPQMixed, 0.0, nullptr);
+    cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRRMixed, fin_count);
     count_launch();
-    cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRMixed, 0.0, nullptr); count_launch();
     // reliable update (every kernel below is a no-op unless state->update)
     flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K.u, state, 0); count_launch();
     {
@@ -820,13 +852,17 @@ struct tp3d_solver {
       r.gate = &state->update;
       rc |= fine<double, kModeResid>(r);
     }
-    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, done, &state->update); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRHi, 0.0, nullptr); count_launch();
+    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, done, &state->update, state, kFinRRHi,
+                                           fin_count);
+    count_launch();
     demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K.r, state, 0); count_launch();
     clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
-    float* z = vcycle<float>(0, K.r, done, &rc);
-    dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr); count_launch();
-    finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZMixed, 0.0, nullptr); count_launch();
+    bool dot_done = false;
+    float* z = vcycle<float>(0, K.r, done, &rc, false, kFinRZMixed, &dot_done);
+    if (!dot_done) {
+      dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZMixed, fin_count);
+      count_launch();
+    }
     cg_p_kernel<float><<<nb, 256, 0, st>>>(ndof, z, K.p, state, 0); count_launch();
     TP3D_CHECK_LAUNCH();
     return rc;
@@ -1015,6 +1051,9 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       o.max_iterations < 1 || !(o.rtol > 0.0) || o.coarsest_max_dofs < 1 || o.max_levels < 1 ||
       !(o.cheb_ratio > 1.0) || o.power_iterations < 2 || !(o.reliable_delta > 0.0 && o.reliable_delta < 1.0))
     return fail(TP3D_ERR_ARG, "invalid solver options");
+  if (o.smoother != 1 && o.pre_sweeps != o.post_sweeps)
+    return fail(TP3D_ERR_ARG, "pre_sweeps and post_sweeps must be equal: the Chebyshev V-cycle preconditions CG and "
+                              "must stay symmetric");
   if (o.omega <= 0.0) o.omega = 0.6;
   s->mixed = o.precision == TP3D_PRECISION_MIXED;
   const bool mixed = s->mixed;
@@ -1077,6 +1116,8 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     if (!s->cyc_blocks64 || !s->cyc_blocks32 || !s->cyc_bar) s->cyc_L0 = 0;
   }
   s->partials = s->alloc<double>(kMaxPartials);
+  s->fin_count = s->alloc<unsigned int>(1);
+  if (s->fin_count) cudaMemset(s->fin_count, 0, sizeof(unsigned int));
   s->state = s->alloc<PcgState>(1);
   unsigned int* cnt = s->alloc<unsigned int>(4);
   if (!s->partials || !s->state || !cnt) return fail(TP3D_ERR_CUDA, "allocation failed");

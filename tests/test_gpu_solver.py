@@ -148,7 +148,9 @@ def test_fused_coarse_cycle_matches_per_phase_launches(P, dims, smoother, prec):
 
     nx, ny, nz = dims
     KE = P.lk_H8(elem_size=1.0)
-    rho, free, fmask = _problem(nx, ny, nz, seed=3, lo=0.05 if smoother else 0.0)
+    # damped Jacobi needs a mild contrast to converge in few iterations; long
+    # runs amplify rounding differences between otherwise identical paths
+    rho, free, fmask = _problem(nx, ny, nz, seed=3, lo=0.3 if smoother else 0.0)
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
     its, Us = [], []
     for fused in (0, 65536):
