@@ -204,7 +204,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * coarsest-inverse fallback flag, lambda_max(Dinv A) of the fine level, residual-floor flag,
  * FP64-fallback flag (mixed), fine form of the FP64 operator and of the FP32 operator
  * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent), first level of the fused
- * coarse cycle (0 none).  Returns the count written. */
+ * coarse cycle (0 none), 1 when the CG loop runs on the device (one graph launch per
+ * solve) rather than host-polled.  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 #ifdef __cplusplus

@@ -20,6 +20,24 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
 
 __global__ void clear_update_kernel(PcgState* st) { st->update = 0; }
 
+// Conditions of the device-side CG loop (CUDA graph conditional nodes).
+// Reliable-update branch: a pending update on a running solve.
+__global__ void set_update_cond_kernel(cudaGraphConditionalHandle h, const PcgState* st) {
+  const bool go = *(volatile const int*)&st->done == 0 && *(volatile const int*)&st->update != 0;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Iteration loop: continue while the solve runs.  The loop also counts its
+// own passes and stops after `limit` of them, so it ends even if no kernel of
+// the body ever updated the state.
+__global__ void set_loop_cond_kernel(cudaGraphConditionalHandle h, const PcgState* st, unsigned int* passes,
+                                     unsigned int limit) {
+  const unsigned int n = *passes + 1u;
+  *passes = n;
+  const bool go = *(volatile const int*)&st->done == 0 && n < limit;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 // a . b into per-block partials; with fin_count, the last block applies op to st.
 template <typename T>
 __global__ void dot_kernel(long long n, const T* __restrict__ a, const T* __restrict__ b, double* partials,

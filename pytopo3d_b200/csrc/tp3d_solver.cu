@@ -56,6 +56,10 @@ struct KrylovVec {
   T *u = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
   cudaGraphExec_t graph = nullptr;
   long long graph_kernels = 0;
+  // device-side loop (conditional nodes): kernels per pass, and in the
+  // reliable-update branch
+  bool loop = false;
+  long long branch_kernels = 0;
 };
 
 struct Tile {
@@ -222,6 +226,12 @@ struct tp3d_solver {
 
   double* partials = nullptr;
   unsigned int* fin_count = nullptr;  // arrivals of the reduction in flight (last_block_finalize)
+  // device-side CG loop (capture_loop)
+  bool loop_ok = true, in_loop_capture = false, branch_ok = true;
+  long long branch_count = 0;
+  cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
+  unsigned int* loop_passes = nullptr;
+  unsigned int* loop_pass_host = nullptr;
   PcgState* state = nullptr;
   PcgState* state_host = nullptr;  // two pinned slots
   Tile tile;
@@ -257,6 +267,8 @@ struct tp3d_solver {
     if (K32.graph) cudaGraphExecDestroy(K32.graph);
     for (void* p : allocs) cudaFree(p);
     if (state_host) cudaFreeHost(state_host);
+    if (loop_pass_host) cudaFreeHost(loop_pass_host);
+    if (st_branch) cudaStreamDestroy(st_branch);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     if (st) cudaStreamDestroy(st);
@@ -649,9 +661,138 @@ struct tp3d_solver {
     return TP3D_OK;
   }
 
+  // The CG iteration as the body of a device-side while loop (a CUDA graph
+  // WHILE node whose condition set_loop_cond_kernel sets at the end of each
+  // pass); a reliable-update branch inside the body becomes an IF node
+  // (update_branch).  One graph launch then runs the whole solve with no host
+  // round trip.  Returns false when the graph cannot be built this way; the
+  // caller then captures the plain iteration and polls.
+  template <typename T, class Body>
+  bool capture_loop(KrylovVec<T>& K, Body body) {
+    if (K.graph) return true;
+    if (!loop_ok) return false;
+    cudaGraph_t G = nullptr;
+    bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+    cudaGraphConditionalHandle hw = 0;
+    ok = ok && cudaGraphConditionalHandleCreate(&hw, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hw;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    ok = ok && cudaGraphAddNode(&wnode, G, nullptr, 0, &cp) == cudaSuccess;
+    bool capturing = false;
+    long long nk = 0;
+    int rc = TP3D_OK;
+    if (ok) {
+      cudaGraph_t B = cp.conditional.phGraph_out[0];
+      capturing = cudaStreamBeginCaptureToGraph(st, B, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                  cudaSuccess;
+      ok = capturing;
+    }
+    if (ok) {
+      t_capture_count = &nk;
+      in_loop_capture = true;
+      branch_count = 0;
+      rc = body();
+      set_loop_cond_kernel<<<1, 1, 0, st>>>(hw, state, loop_passes, (unsigned int)o.max_iterations + 16u);
+      ++nk;
+      in_loop_capture = false;
+      t_capture_count = nullptr;
+    }
+    if (capturing) {
+      cudaGraph_t out = nullptr;
+      ok = cudaStreamEndCapture(st, &out) == cudaSuccess && ok;
+    }
+    ok = ok && rc == TP3D_OK && branch_ok && cudaGraphInstantiate(&K.graph, G, 0) == cudaSuccess;
+    if (G) cudaGraphDestroy(G);
+    cudaGetLastError();  // clear a failed attempt's error state
+    if (!ok) {
+      if (K.graph) cudaGraphExecDestroy(K.graph);
+      K.graph = nullptr;
+      loop_ok = false;
+      return false;
+    }
+    K.loop = true;
+    K.graph_kernels = nk;
+    K.branch_kernels = branch_count;
+    return true;
+  }
+
+  // Kernels of the reliable update: inside a loop capture they form the body
+  // of an IF node on set_update_cond_kernel's condition; otherwise they are
+  // launched directly (each gated on state->update itself).
+  template <class Branch>
+  int update_branch(Branch branch) {
+    if (!in_loop_capture) return branch();
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle h = 0;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&h, capg, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+      branch_ok = false;
+      return TP3D_ERR_CUDA;
+    }
+    set_update_cond_kernel<<<1, 1, 0, st>>>(h, state);
+    count_launch();
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd) != cudaSuccess ||
+        cudaGraphAddNode(&node, capg, deps, nd, &cp) != cudaSuccess ||
+        cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) {
+      branch_ok = false;
+      return TP3D_ERR_CUDA;
+    }
+    // the branch body, captured on the second stream
+    std::swap(st, st_branch);
+    int rc = TP3D_OK;
+    if (cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      branch_ok = false;
+      rc = TP3D_ERR_CUDA;
+    } else {
+      long long* outer = t_capture_count;
+      long long nb = 0;
+      t_capture_count = &nb;
+      rc = branch();
+      t_capture_count = outer;
+      cudaGraph_t out = nullptr;
+      if (cudaStreamEndCapture(st, &out) != cudaSuccess) {
+        branch_ok = false;
+        rc = TP3D_ERR_CUDA;
+      }
+      branch_count += nb;
+    }
+    std::swap(st, st_branch);
+    return rc;
+  }
+
+  // One launch of the loop graph; the pass count and reliable updates of the
+  // run feed the launch counter.
+  template <typename T>
+  int replay_loop(KrylovVec<T>& K) {
+    TP3D_CHECK(cudaMemsetAsync(loop_passes, 0, sizeof(unsigned int), st));
+    TP3D_CHECK(cudaGraphLaunch(K.graph, st));
+    unsigned int passes = 0;
+    TP3D_CHECK(cudaMemcpyAsync(state_host, state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+    TP3D_CHECK(cudaMemcpyAsync(loop_pass_host, loop_passes, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    TP3D_CHECK(cudaStreamSynchronize(st));
+    passes = *loop_pass_host;
+    add_launches((long long)passes * K.graph_kernels + (long long)state_host[0].updates * K.branch_kernels);
+    return TP3D_OK;
+  }
+
   // Replay the iteration graph until the device stop flag is set (two-deep polling).
   template <typename T>
   int replay(KrylovVec<T>& K, int max_iters) {
+    if (K.loop) return replay_loop<T>(K);
     const int chunk = 4;
     int launched = 0, which = 0, status = TP3D_OK;
     bool pending = false;
@@ -734,7 +875,9 @@ struct tp3d_solver {
   int pcg64_run(const double* F, double rtol, int max_iters) {
     const long long nn = g.nnode(), ndof = 3 * nn;
     const int nb = grid_blocks(ndof);
-    int rc = capture<double>(K64, [&]() { return pcg64_iteration(); });
+    int rc = TP3D_OK;
+    if (!capture_loop<double>(K64, [&]() { return pcg64_iteration(); }))
+      rc = capture<double>(K64, [&]() { return pcg64_iteration(); });
     if (rc) return rc;
     PcgState init{};
     init.max_iters = max_iters;
@@ -841,22 +984,24 @@ struct tp3d_solver {
     int rc = fine<float, kModeCgQ>(io);
     cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRRMixed, fin_count);
     count_launch();
-    // reliable update (every kernel below is a no-op unless state->update)
-    flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K.u, state, 0); count_launch();
-    {
+    // reliable update (each kernel is also gated on state->update itself)
+    rc |= update_branch([&]() {
+      int brc = TP3D_OK;
+      flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K.u, state, 0); count_launch();
       OpIO<double> r;
       r.u = u64;
       r.out = r64;
       r.b = F_capture;
       r.done = done;
       r.gate = &state->update;
-      rc |= fine<double, kModeResid>(r);
-    }
-    dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, done, &state->update, state, kFinRRHi,
-                                           fin_count);
-    count_launch();
-    demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K.r, state, 0); count_launch();
-    clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
+      brc |= fine<double, kModeResid>(r);
+      dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, done, &state->update, state, kFinRRHi,
+                                             fin_count);
+      count_launch();
+      demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K.r, state, 0); count_launch();
+      clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
+      return brc;
+    });
     bool dot_done = false;
     float* z = vcycle<float>(0, K.r, done, &rc, false, kFinRZMixed, &dot_done);
     if (!dot_done) {
@@ -872,7 +1017,9 @@ struct tp3d_solver {
     const long long nn = g.nnode(), ndof = 3 * nn;
     const int nb = grid_blocks(ndof);
     last_floor = false;
-    int rc = capture<float>(K32, [&]() { return mixed_iteration(); });
+    int rc = TP3D_OK;
+    if (!capture_loop<float>(K32, [&]() { return mixed_iteration(); }))
+      rc = capture<float>(K32, [&]() { return mixed_iteration(); });
     if (rc) return rc;
     PcgState init{};
     init.max_iters = o.max_iterations;
@@ -1118,6 +1265,10 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   s->partials = s->alloc<double>(kMaxPartials);
   s->fin_count = s->alloc<unsigned int>(1);
   if (s->fin_count) cudaMemset(s->fin_count, 0, sizeof(unsigned int));
+  s->loop_passes = s->alloc<unsigned int>(1);
+  if (cudaMallocHost(&s->loop_pass_host, sizeof(unsigned int)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->st_branch, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(TP3D_ERR_CUDA, "solver setup failed");
   s->state = s->alloc<PcgState>(1);
   unsigned int* cnt = s->alloc<unsigned int>(4);
   if (!s->partials || !s->state || !cnt) return fail(TP3D_ERR_CUDA, "allocation failed");
@@ -1487,7 +1638,7 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0,
                            s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
                            s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0,
-                           (double)s->cyc_L0};
+                           (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

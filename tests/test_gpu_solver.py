@@ -125,6 +125,7 @@ def test_mixed_precision_matches_fp64(P, dims, opts):
         assert rtol == (1e-10 if prec == "fp64" else opts.get("rtol", 1e-6))
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
+        assert s.stats()["device_loop"] == 1.0  # one graph launch per solve, no host polling
         # 1e-9 void pockets put an attainable floor on the true residual; the
         # solver accepts it only once restarts / reliable updates stop gaining
         assert s.last_relres <= rtol or (s.stats()["residual_floor"] and s.last_relres <= max(rtol, 1e-7))
