@@ -50,6 +50,7 @@ class SolverOpts(C.Structure):
         ("fine_operator", i32),
         ("fused_cycle_dofs", i32),
         ("galerkin", i32),
+        ("coarse_sweeps", i32),
     ]
 
 

@@ -56,7 +56,7 @@ enum ApplyMode : int {
   kModeChebFirst = 4,  // d = c0 Dinv (b - K u); out = u + d
   kModeChebStep = 5,   // d = c1 d + c2 Dinv (b - K u); out = u + d
   kModeDinvApply = 6,  // out = Dinv K u (power iteration for lambda_max(Dinv K))
-  kModeChebStepDot = 7,  // as kModeChebStep, and partials += b . out (the CG's r . z)
+  kModeChebStepDot = 7,  // Chebyshev step (first step when io.step == 0), and partials += b . out
 };
 
 // Inputs / outputs shared by every operator kernel.
@@ -134,12 +134,18 @@ __device__ __forceinline__ void op_epilogue(const OpIO<T>& io, long long i, bool
     const T dd = fx ? T(0) : (T)io.coef[0] * in.dinv * (in.b - kv);
     io.d[i] = dd;
     io.out[i] = own + dd;
-  } else if (MODE == kModeChebStep || MODE == kModeChebStepDot) {
+  } else if (MODE == kModeChebStep) {
     const T dd = fx ? T(0) : (T)io.coef[2 * io.step] * in.d + (T)io.coef[2 * io.step + 1] * in.dinv * (in.b - kv);
+    io.d[i] = dd;
+    io.out[i] = own + dd;
+  } else if (MODE == kModeChebStepDot) {
+    T dd;
+    if (io.step == 0) dd = fx ? T(0) : (T)io.coef[0] * in.dinv * (in.b - kv);
+    else dd = fx ? T(0) : (T)io.coef[2 * io.step] * in.d + (T)io.coef[2 * io.step + 1] * in.dinv * (in.b - kv);
     io.d[i] = dd;
     const T z = own + dd;
     io.out[i] = z;
-    if (MODE == kModeChebStepDot) part += (double)in.b * (double)z;
+    part += (double)in.b * (double)z;
   } else {  // kModeDinvApply
     io.out[i] = fx ? T(0) : in.dinv * kv;
   }

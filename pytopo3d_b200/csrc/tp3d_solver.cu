@@ -476,8 +476,8 @@ struct tp3d_solver {
 
   // ---------------- V-cycle ----------------
   template <typename T>
-  // dot_op >= 0: the last step is a Chebyshev step (s >= 1) that also reduces
-  // b . out and applies finalize op dot_op (the caller checked it applies).
+  // dot_op >= 0: the last step is a Chebyshev step that also reduces b . out
+  // and applies finalize op dot_op (the caller checked it applies).
   int smooth_steps(int L, int first_step, int nsteps, int* cur, const T* b, const int* done, int dot_op = -1) {
     auto& lv = levels<T>()[L];
     int rc = TP3D_OK;
@@ -532,8 +532,8 @@ struct tp3d_solver {
     p.lv[L].b = const_cast<T*>(b);
     p.L0 = L;
     p.Lc = nlev - 1;
-    p.pre = o.pre_sweeps;
-    p.post = o.post_sweeps;
+    p.pre = pre_sweeps(L);
+    p.post = post_sweeps(L);
     p.cheb = o.smoother != 1 ? 1 : 0;
     p.omega = (T)o.omega;
     p.cn = cn;
@@ -554,7 +554,7 @@ struct tp3d_solver {
     cfg.numAttrs = 1;
     if (cudaLaunchKernelEx(&cfg, coarse_cycle_kernel<T>, p) != cudaSuccess) *rc = TP3D_ERR_CUDA;
     count_launch();
-    return L == nlev - 1 ? lvs[L].x[0] : lvs[L].x[cycle_final_buffer(o.pre_sweeps, o.post_sweeps)];
+    return L == nlev - 1 ? lvs[L].x[0] : lvs[L].x[cycle_final_buffer(pre_sweeps(L), post_sweeps(L))];
   }
 
   // Cooperative grid for the coarse cycle from level L: enough blocks for
@@ -568,6 +568,10 @@ struct tp3d_solver {
     const long long need = (3 * grids[L].nnode() + 255) / 256;
     return (int)std::max<long long>(1, std::min<long long>(need, (long long)occ * nsm));
   }
+
+  // smoothing degrees of level L (coarse_sweeps > 0 overrides both on levels >= 1)
+  int pre_sweeps(int L) const { return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.pre_sweeps; }
+  int post_sweeps(int L) const { return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.post_sweeps; }
 
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
@@ -604,7 +608,7 @@ struct tp3d_solver {
                                                                lv.x[cur], cheb ? lv.d : nullptr, done);
       count_launch();
     }
-    *rc |= smooth_steps<T>(L, 1, o.pre_sweeps - 1, &cur, b, done);
+    *rc |= smooth_steps<T>(L, 1, pre_sweeps(L) - 1, &cur, b, done);
     {
       OpIO<T> io;
       io.u = lv.x[cur];
@@ -632,8 +636,8 @@ struct tp3d_solver {
     prolong_add_kernel<T><<<plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1), 256, 0, st>>>(gl, gn, xc, fix[L],
                                                                                              lv.x[cur], done);
     count_launch();
-    const bool dot_here = dot_op >= 0 && o.smoother != 1 && o.post_sweeps >= 2;
-    *rc |= smooth_steps<T>(L, 0, o.post_sweeps, &cur, b, done, dot_here ? dot_op : -1);
+    const bool dot_here = dot_op >= 0 && o.smoother != 1 && post_sweeps(L) >= 1;
+    *rc |= smooth_steps<T>(L, 0, post_sweeps(L), &cur, b, done, dot_here ? dot_op : -1);
     if (dot_here && dot_done) *dot_done = true;
     if (cudaGetLastError() != cudaSuccess) *rc = TP3D_ERR_CUDA;
     return lv.x[cur];
@@ -1165,13 +1169,13 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->precision = TP3D_PRECISION_FP64;
   o->max_iterations = 2000;
   o->rtol = 1e-10;
-  o->pre_sweeps = 2;
-  o->post_sweeps = 2;
+  o->pre_sweeps = 1;
+  o->post_sweeps = 1;
   o->omega = 0.6;
   o->coarsest_max_dofs = 500;
   o->max_levels = 12;
   o->smoother = 0;
-  o->cheb_ratio = 15.0;
+  o->cheb_ratio = 30.0;
   o->power_iterations = 12;
   o->inner_density = 0;
   o->reliable_delta = 0.05;
@@ -1179,6 +1183,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->fine_operator = 0;
   o->fused_cycle_dofs = 0;
   o->galerkin = 0;
+  o->coarse_sweeps = 2;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1198,6 +1203,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       o.max_iterations < 1 || !(o.rtol > 0.0) || o.coarsest_max_dofs < 1 || o.max_levels < 1 ||
       !(o.cheb_ratio > 1.0) || o.power_iterations < 2 || !(o.reliable_delta > 0.0 && o.reliable_delta < 1.0))
     return fail(TP3D_ERR_ARG, "invalid solver options");
+  if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.smoother != 1 && o.pre_sweeps != o.post_sweeps)
     return fail(TP3D_ERR_ARG, "pre_sweeps and post_sweeps must be equal: the Chebyshev V-cycle preconditions CG and "
                               "must stay symmetric");
