@@ -181,13 +181,20 @@ def barrier(dist):
 
 
 def max_over_ranks(v, dist):
+    """Largest value over the ranks (the job's time is its slowest replica's)."""
     if dist is None:
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, seconds, world):
+    """Whole-job throughput of `world` independent replicas at the max-over-ranks time."""
+    return world * units_per_rank / seconds
 
 
 def cpu_reference_sample(steps=1):
@@ -311,7 +318,7 @@ def main():
     ndof = 3 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
     nele = NELX * NELY * NELZ
     steps = main_r["steps"]
-    rate = world * steps / (main_r["ms"] / 1e3)
+    rate = job_rate(steps, main_r["ms"] / 1e3, world)
 
     # end-to-end through the public API with host buffers (pinned H2D of x, D2H of x_new + c)
     x_host = loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
@@ -325,7 +332,7 @@ def main():
         x_host, c_host = loop.step_host(x_host)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e_rate = world * e_steps / e2e_s
+    e2e_rate = job_rate(e_steps, e2e_s, world)
 
     # roofline of the dominant kernel (fine-level operator apply)
     peak, peak_kind = peaks()

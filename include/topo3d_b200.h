@@ -168,6 +168,9 @@ typedef struct tp3d_solver_opts {
   int coarse_sweeps;    /* smoother degree (before and after) on levels >= 1; 0: pre/post_sweeps.
                            Defaults (fine degree 1, coarse degree 2, interval ratio 30) are the
                            fastest measured on the 128x64x64 cantilever in both precisions. */
+  int device_loop;      /* 1: the CG loop runs on the device (one CUDA graph per solve with a
+                           conditional WHILE node); 0: the host replays a one-iteration graph and
+                           polls the stop flag (profilers see the loop's kernels only then) */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

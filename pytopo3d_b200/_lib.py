@@ -51,6 +51,7 @@ class SolverOpts(C.Structure):
         ("fused_cycle_dofs", i32),
         ("galerkin", i32),
         ("coarse_sweeps", i32),
+        ("device_loop", i32),
     ]
 
 

@@ -415,6 +415,83 @@ __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const dou
   if (threadIdx.x == 0) *status = bad;
 }
 
+// Gauss-Jordan inverse of a small SPD matrix (n <= 160) held in registers: one
+// block of 16 x 32 threads, thread (w, l) owns the 10 x 5 entries (w + 16 r,
+// l + 32 c).  Per pivot step the owners of row k and column k publish them in
+// shared memory (double-buffered, one barrier per step) and every thread
+// updates its entries in registers.  Same arithmetic as
+// dense_gj_inverse_kernel.  *status = 0 ok, k+1 if pivot k was not positive.
+constexpr int kGjRegMaxN = 160;
+
+__global__ void __launch_bounds__(512, 1) dense_gj_inverse_reg_kernel(int n, const double* __restrict__ D, double* Inv,
+                                                                      int* status) {
+  constexpr int R = 10, C = 5;
+  __shared__ double rowk[2][kGjRegMaxN], colk[2][kGjRegMaxN];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  double a[R][C];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const int i = w + 16 * r, j = l + 32 * c;
+      a[r][c] = (i < n && j < n) ? D[(size_t)i * n + j] : 0.0;
+    }
+  int bad = 0;
+  for (int k = 0; k < n; ++k) {
+    const int buf = k & 1;
+    // owners of row k (warp k % 16, r = k / 16) and of column k (lane k % 32,
+    // c = k / 32) publish them; selects keep every index compile-time
+    if (w == (k & 15)) {
+      const int kr = k >> 4;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v = (r == kr) ? a[r][c] : v;
+        rowk[buf][l + 32 * c] = v;
+      }
+    }
+    if (l == (k & 31)) {
+      const int kc = k >> 5;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) v = (c == kc) ? a[r][c] : v;
+        colk[buf][w + 16 * r] = v;
+      }
+    }
+    __syncthreads();
+    const double p = rowk[buf][k];
+    if (!(p > 0.0) && !bad) bad = k + 1;
+    const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
+    double g[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) g[c] = rowk[buf][l + 32 * c];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const bool rk = (w + 16 * r) == k;
+      const double f = colk[buf][w + 16 * r] * pk;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const bool ck = (l + 32 * c) == k;
+        double v = a[r][c] - f * g[c];
+        if (ck) v = -f;
+        if (rk) v = ck ? pk : g[c] * pk;
+        a[r][c] = v;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const int i = w + 16 * r, j = l + 32 * c;
+      if (i < n && j < n) Inv[(size_t)i * n + j] = a[r][c];
+    }
+  if (threadIdx.x == 0) *status = bad;
+}
+
 template <typename T>
 __global__ void dense_matvec_kernel(int n, const T* __restrict__ Inv, const T* __restrict__ b, T* x, const int* done) {
   if (done && *(volatile const int*)done) return;

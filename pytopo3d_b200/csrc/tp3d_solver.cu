@@ -674,7 +674,7 @@ struct tp3d_solver {
   template <typename T, class Body>
   bool capture_loop(KrylovVec<T>& K, Body body) {
     if (K.graph) return true;
-    if (!loop_ok) return false;
+    if (!loop_ok || !o.device_loop) return false;
     cudaGraph_t G = nullptr;
     bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
     cudaGraphConditionalHandle hw = 0;
@@ -1184,6 +1184,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->fused_cycle_dofs = 0;
   o->galerkin = 0;
   o->coarse_sweeps = 2;
+  o->device_loop = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1500,13 +1501,15 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
         dense_shift_kernel<<<s->grid_blocks(n), 256, 0, st>>>(n, s->cdense, shift);
         count_launch();
       }
-      {
-        const int in_smem = n <= 160 ? 1 : 0;
-        const size_t smem = ((in_smem ? (size_t)n * n : 0) + 2 * (size_t)n) * sizeof(double);
+      if (n <= kGjRegMaxN) {
+        dense_gj_inverse_reg_kernel<<<1, 512, 0, st>>>(n, s->cdense, s->cinv64, s->cstatus);
+        count_launch();
+      } else {
+        const size_t smem = 2 * (size_t)n * sizeof(double);
         if (smem > 48 * 1024)
           TP3D_CHECK(cudaFuncSetAttribute(dense_gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-        dense_gj_inverse_kernel<<<1, 1024, smem, st>>>(n, s->cdense, s->cinv64, in_smem, s->cstatus);
+        dense_gj_inverse_kernel<<<1, 1024, smem, st>>>(n, s->cdense, s->cinv64, 0, s->cstatus);
         count_launch();
       }
       TP3D_CHECK_LAUNCH();

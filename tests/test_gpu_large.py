@@ -1,0 +1,47 @@
+"""The large single design: a 256x128x128 cantilever (4.19 M elements,
+12.8 M DOFs), volfrac 0.2, rmin 4.5, beta 1, the mixed-precision solver.
+
+The reference cannot set this problem up (its filter lists and scatter map
+need more host memory than the machine has), so the checks are properties
+that hold at any size: the OC update meets the volume target, the compliance
+is finite and falls over the first iterations, and one mixed-precision solve
+agrees with an FP64 solve of the same system within 1e-6 (compliance).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def test_large_cantilever_runs_and_meets_the_volume_target():
+    import bench
+    from pytopo3d_b200.optimizer import SimpLoop
+    from pytopo3d_b200.solver import HexSolver
+    from pytopo3d_b200.stiffness import lk_H8
+
+    nelx, nely, nelz = 256, 128, 128
+    shape, solid, void, F, fixed = bench.workload(nelx, nely, nelz)
+    KE = lk_H8(elem_size=1.0)
+    loop = SimpLoop(nelx, nely, nelz, 0.2, 3.0, 4.5, KE, F, fixed, solid, void, precision="mixed")
+    loop.set_beta(1.0)
+    cs = []
+    for _ in range(3):
+        st = loop.step()
+        cs.append(float(st[0]))
+        vol = float(st[2])
+        assert abs(vol - loop.target) <= 1e-6 * loop.target + 1.0  # projected free volume at the target
+    assert all(np.isfinite(cs)) and cs[2] < cs[0]
+    # one solve of the current design: mixed vs FP64
+    S = loop.S
+    ref = HexSolver(nelx, nely, nelz, KE, fixed, precision="fp64")
+    ref.set_density(S.rho_p, 3.0)
+    Ur = ref.solve(S.F[0], S.U[0].clone())
+    loop.solver.set_density(S.rho_p, 3.0)
+    Um = loop.solver.solve(S.F[0], S.U[0].clone())
+    c_r = float(Ur @ ref.apply(Ur))
+    c_m = float(Um @ ref.apply(Um))
+    assert abs(c_m - c_r) <= 1e-6 * abs(c_r)
+    ref.close()
+    loop.close()
