@@ -20,6 +20,17 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
 
 __global__ void clear_update_kernel(PcgState* st) { st->update = 0; }
 
+// Linear extrapolation of successive solutions as the next initial guess:
+// U <- 2 U - U_prev and U_prev <- U (old), or only U_prev <- U when there is no
+// history yet.
+__global__ void warm_start_kernel(long long n, double* U, double* U_prev, int have_prev) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double u = U[i];
+    if (have_prev) U[i] = 2.0 * u - U_prev[i];
+    U_prev[i] = u;
+  }
+}
+
 // Conditions of the device-side CG loop (CUDA graph conditional nodes).
 // Reliable-update branch: a pending update on a running solve.
 __global__ void set_update_cond_kernel(cudaGraphConditionalHandle h, const PcgState* st) {

@@ -1634,6 +1634,16 @@ extern "C" int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, do
   return s->leave();
 }
 
+extern "C" int tp3d_warm_start(double* U, double* U_prev, long long n, int have_prev, void* stream) {
+  if (!U || !U_prev || n < 0) return TP3D_ERR_ARG;
+  if (n == 0) return TP3D_OK;
+  const int nb = (int)std::min<long long>((n + 255) / 256, 1184);
+  warm_start_kernel<<<nb, 256, 0, (cudaStream_t)stream>>>(n, U, U_prev, have_prev);
+  count_launch();
+  TP3D_CHECK_LAUNCH();
+  return TP3D_OK;
+}
+
 extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
   if (!s || !out) return TP3D_ERR_ARG;
   std::vector<double> lam(s->nlev, 0.0);

@@ -80,6 +80,8 @@ class SimpState:
         self.dc_acc = z()
         self.c_dev = torch.zeros(2, dtype=torch.float64, device=device())
         self.U = torch.zeros_like(F)
+        self.U_prev = torch.zeros_like(F)  # last solutions, for the extrapolated initial guess
+        self.n_solved = 0
         self.sens_scratch = torch.empty(
             _lib.lib().tp3d_sensitivity_scratch_bytes(H.nelx, H.nely, H.nelz), dtype=torch.uint8,
             device=device())
@@ -91,6 +93,11 @@ class SimpState:
                             self.rho_p if rho_p is None else rho_p,
                             self.dproj if dproj is None else dproj)
 
+    def new_stage(self):
+        """A projection change moves the physical design at once: the next solve
+        starts from the last solution, not from an extrapolation across the jump."""
+        self.n_solved = min(self.n_solved, 1)
+
     def sensitivities(self, rho_p, dproj):
         """Solve every load case, then fused energy / compliance / chain rule."""
         L = _lib.lib()
@@ -98,6 +105,8 @@ class SimpState:
         self.solver.set_density(rho_p, self.penal)
         iters = 0
         for k in range(self.F.shape[0]):
+            _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
+                                         1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
             self.solver.solve(self.F[k], self.U[k])
             iters += self.solver.last_iterations
             dst_dc = self.dc_dx if k == 0 else self.dc_acc
@@ -110,6 +119,7 @@ class SimpState:
             if k > 0:
                 self.dc_dx += self.dc_acc
                 self.c_dev[0] += self.c_dev[1]
+        self.n_solved += 1
         return iters
 
 
@@ -152,6 +162,7 @@ class SimpLoop:
     def set_beta(self, beta):
         self.beta = float(beta)
         self.S.project(self.x, self.beta, self.eta)
+        self.S.new_stage()
 
     def step(self):
         """One loop body: solve, sensitivities, OC update, re-projection.
@@ -338,6 +349,7 @@ def top3d(
         logger.info("Starting projection stage: beta=%g", beta)
         change, stage_loop, c_prev = float("inf"), 0, float("nan")
         S.project(x, beta, projection_eta)
+        S.new_stage()
         vmin, vmax = bounds(beta)
         within = vmin - 1.0e-10 <= volfrac <= vmax + 1.0e-10
         if volfrac < vmin - 1.0e-10:
