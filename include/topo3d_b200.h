@@ -200,9 +200,11 @@ int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
 int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
 
 /* Average device time (ms) of the fine-level operator kernel over `launches`
- * back-to-back launches on the solver's stream, timed with CUDA events around
- * them (fp32 != 0: the mixed-precision FP32/BF16 kernel).  Measurement helper
- * for the roofline figure; no reference counterpart. */
+ * back-to-back launches on the solver's stream, timed with one pair of CUDA
+ * events, the launches rotating over input/output vectors that together exceed
+ * twice L2 so that each reads its input from HBM (fp32 != 0: the mixed form's
+ * FP32 kernel).  Measurement helper for the roofline figure; no reference
+ * counterpart. */
 int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch);
 
 /* Diagnostics of the last solve, in this order: levels, CG iterations, reliable updates

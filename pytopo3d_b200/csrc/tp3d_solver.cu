@@ -381,10 +381,55 @@ struct tp3d_solver {
   int fine_wht(int mode, const OpIO<T>& io) {
     return fine_wht_tile<T>(mode, io, wtile<T>());
   }
+  // Average time of `launches` back-to-back Apply-mode launches of the fine
+  // operator (current form) rotating over input/output vector pairs that
+  // together exceed twice L2 (at most 64 pairs), so each launch reads cold
+  // inputs; one warm-up pass over all pairs first, events on the solver's
+  // stream.  The vectors are allocated for the measurement and freed after it.
+  template <typename T>
+  int time_fine_cold(int launches, double* ms_out) {
+    constexpr size_t kColdBytes = (size_t)256 << 20;
+    const long long ndof = 3 * g.nnode();
+    const size_t pair_bytes = (size_t)ndof * sizeof(T) * 2;
+    const int npairs =
+        (int)std::min<size_t>(64, std::max<size_t>(2, (kColdBytes + pair_bytes - 1) / pair_bytes));
+    unsigned char* buf = nullptr;
+    if (cudaMalloc(&buf, (size_t)npairs * pair_bytes) != cudaSuccess) {
+      tp3d_set_last_error("timing buffers: allocation failed");
+      return TP3D_ERR_CUDA;
+    }
+    struct Free {
+      unsigned char* p;
+      ~Free() { cudaFree(p); }
+    } guard{buf};
+    TP3D_CHECK(cudaMemsetAsync(buf, 0, (size_t)npairs * pair_bytes, st));
+    auto launch = [&](int k) -> int {
+      unsigned char* base = buf + (size_t)(k % npairs) * pair_bytes;
+      OpIO<T> io;
+      io.u = (const T*)base;
+      io.out = (T*)base + ndof;
+      return fine<T, kModeApply>(io);
+    };
+    int rc = TP3D_OK;
+    for (int k = 0; k < npairs && rc == TP3D_OK; ++k) rc = launch(k);
+    cudaEvent_t a, b;
+    TP3D_CHECK(cudaEventCreate(&a));
+    TP3D_CHECK(cudaEventCreate(&b));
+    TP3D_CHECK(cudaEventRecord(a, st));
+    for (int k = 0; k < launches && rc == TP3D_OK; ++k) rc = launch(k);
+    TP3D_CHECK(cudaEventRecord(b, st));
+    TP3D_CHECK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    TP3D_CHECK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms_out = ms / launches;
+    return rc;
+  }
+
   // Fine operator form for precision T: the dense-KE kernel or one of the
   // Walsh-Hadamard variants, whichever runs the Apply mode fastest on this
-  // grid (2 warm-up launches, then the best of 3 rounds of 5, events on the
-  // solver stream);
+  // grid with cold inputs (time_fine_cold, 12 launches each);
   // fine_operator = 1 / 2 restricts the choice to one form.
   template <typename T>
   int choose_fine_form() {
@@ -392,39 +437,7 @@ struct tp3d_solver {
     WhtTile& wt = sizeof(T) == 8 ? wt64 : wt32;
     use = false;
     if (!wht_ok) return TP3D_OK;
-    const T* in;
-    T* out;
-    if constexpr (sizeof(T) == 8) {
-      in = u64;
-      out = pw[0];
-    } else {
-      in = K32.p;
-      out = K32.q;
-    }
-    TP3D_CHECK(cudaMemsetAsync((void*)in, 0, 3 * g.nnode() * sizeof(T), st));
-    cudaEvent_t a, b;
-    TP3D_CHECK(cudaEventCreate(&a));
-    TP3D_CHECK(cudaEventCreate(&b));
-    auto time_one = [&](double* ms) -> int {
-      OpIO<T> io;
-      io.u = in;
-      io.out = out;
-      for (int i = 0; i < 2; ++i)
-        if (int rc = fine<T, kModeApply>(io)) return rc;
-      double best = 1e300;
-      for (int round = 0; round < 3; ++round) {
-        TP3D_CHECK(cudaEventRecord(a, st));
-        for (int i = 0; i < 5; ++i)
-          if (int rc = fine<T, kModeApply>(io)) return rc;
-        TP3D_CHECK(cudaEventRecord(b, st));
-        TP3D_CHECK(cudaEventSynchronize(b));
-        float f = 0.f;
-        TP3D_CHECK(cudaEventElapsedTime(&f, a, b));
-        best = std::min(best, (double)f);
-      }
-      *ms = best;
-      return TP3D_OK;
-    };
+    auto time_one = [&](double* ms) -> int { return time_fine_cold<T>(12, ms); };
     double best = 1e300;
     int best_v = -1;
     int rc = TP3D_OK;
@@ -446,8 +459,6 @@ struct tp3d_solver {
         best_v = v;
       }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     if (rc) return rc;
     if (best_v >= 0) {
       if constexpr (sizeof(T) == 8) wt = wht_choose_tile<double, EFromF64>(g, nsm, best_v);
@@ -1105,7 +1116,6 @@ struct tp3d_solver {
     count_launch();
   }
   bool last_fallback = false;
-  unsigned char* flush = nullptr;  // L2 flush buffer of tp3d_solver_time_apply
 };
 
 // KE1[s] = P_s^T KE P_s: interpolation from a coarse element's corners to its
@@ -1592,44 +1602,14 @@ extern "C" int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y) {
   return s->leave();
 }
 
-// Average duration of one fine-operator launch (Apply mode) with a cold L2:
-// a 256 MiB buffer is written between launches and each launch is bracketed
-// by its own pair of events on the solver's stream.
+// Average duration of one fine-operator launch (Apply mode) over back-to-back
+// launches with cold inputs (see time_fine_cold).
 extern "C" int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch) {
   if (!s || !ms_per_launch || launches < 1 || !s->have_density) return TP3D_ERR_ARG;
   if (fp32 && !s->mixed) return TP3D_ERR_ARG;
-  constexpr size_t kFlushBytes = (size_t)256 << 20;
-  if (!s->flush) s->flush = s->alloc<unsigned char>(kFlushBytes);
-  if (!s->flush) return TP3D_ERR_CUDA;
   if (int rc = s->enter()) return rc;
-  cudaEvent_t a, b;
-  TP3D_CHECK(cudaEventCreate(&a));
-  TP3D_CHECK(cudaEventCreate(&b));
-  int rc = TP3D_OK;
-  double total = 0.0;
-  for (int i = -1; i < launches && rc == TP3D_OK; ++i) {  // i = -1: warm-up
-    TP3D_CHECK(cudaMemsetAsync(s->flush, i & 0xff, kFlushBytes, s->st));
-    TP3D_CHECK(cudaEventRecord(a, s->st));
-    if (fp32) {
-      OpIO<float> io;
-      io.u = s->K32.p;
-      io.out = s->K32.q;
-      rc = s->fine<float, kModeApply>(io);
-    } else {
-      OpIO<double> io;
-      io.u = s->u64;
-      io.out = s->pw[0];
-      rc = s->fine<double, kModeApply>(io);
-    }
-    TP3D_CHECK(cudaEventRecord(b, s->st));
-    TP3D_CHECK(cudaEventSynchronize(b));
-    float ms = 0.f;
-    TP3D_CHECK(cudaEventElapsedTime(&ms, a, b));
-    if (i >= 0) total += ms;
-  }
-  *ms_per_launch = total / launches;
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  const int rc = fp32 ? s->time_fine_cold<float>(launches, ms_per_launch)
+                      : s->time_fine_cold<double>(launches, ms_per_launch);
   if (rc) return rc;
   return s->leave();
 }
