@@ -258,7 +258,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply", "batch"],
                     help="step: warm-up + --steps loop bodies only (for launch lists); "
                          "apply: fine-operator launches only (for kernel captures)")
     ap.add_argument("--size", type=int, default=NELX, help="nelx for --mode step/apply (nely = nelz = nelx/2)")
@@ -267,6 +267,8 @@ def main():
     ap.add_argument("--solver-opt", action="append", default=[], metavar="KEY=VALUE",
                     help="further solver options for --mode step/apply (integers or floats)")
     args = ap.parse_args()
+    if args.mode == "batch":
+        return run_batch(args)
     if args.mode != "bench":
         return run_probe(args)
 
@@ -396,6 +398,35 @@ def main():
     loop.close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def run_batch(args):
+    """The batched workload: 64 seeded cantilevers of uneven sizes, each an
+    independent loop on its own stream, 8 host threads; --steps loop bodies per
+    design after --warmup.  The same designs one after another on the default
+    stream are timed beside it.  Prints one JSON line (not the headline bench
+    line)."""
+    import torch
+
+    from pytopo3d_b200.batch import BatchRunner, batched_cantilevers
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    specs = batched_cantilevers(64, seed=0)
+    br = BatchRunner(specs, precision=args.precision, workers=8)
+    br.run(max(1, args.warmup))
+    conc = br.run(args.steps)
+    br.close()
+    seq = BatchRunner(specs, precision=args.precision, workers=1)
+    seq.run(max(1, args.warmup))
+    one = seq.run(args.steps)
+    seq.close()
+    nele = [s.nelx * s.nely * s.nelz for s in specs]
+    print(json.dumps({"mode": "batch", "designs": len(specs), "precision": args.precision, "steps": args.steps,
+                      "elements_total": int(sum(nele)), "elements_min": int(min(nele)),
+                      "elements_max": int(max(nele)), "concurrent_8_threads": conc,
+                      "one_after_another": one,
+                      "speedup": conc["simp_iterations_per_s"] / one["simp_iterations_per_s"]}))
     return 0
 
 

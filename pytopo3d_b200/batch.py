@@ -1,0 +1,174 @@
+"""Many independent SIMP designs at once on one GPU.
+
+A batch of designs of uneven grid sizes (the batched workload: 64 seeded
+cantilevers with random sizes, volume fractions, filter radii, void
+cylinders and load positions) is run as one ``SimpLoop`` per design, each on
+its own CUDA stream, driven by a small pool of host threads.  Every design
+is an independent problem, so nothing is shared between them but the GPU:
+the small designs' launches, which would leave most of the 148 SMs idle one
+at a time, overlap across streams.  (The library calls release the GIL, so
+the host threads run concurrently too.)
+
+The reference runs designs one after another (runners/experiment.py); this
+module has no reference counterpart beyond the per-design loop body, which
+is ``SimpLoop.step`` (optimizer.py:578-696).
+"""
+
+from __future__ import annotations
+
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from ._tensors import device
+from .assembly import build_force_vector, build_supports
+from .obstacles import cylinder_mask_elements
+from .optimizer import SimpLoop, _elements_at_loaded_nodes
+from .stiffness import lk_H8
+
+
+@dataclass
+class DesignSpec:
+    """One cantilever of the batch: grid, volume fraction, filter radius, void
+    cylinders ``(axis, centre_a, centre_b, radius)`` in element units (centre in
+    the two axes perpendicular to ``axis``, in x, y, z order), and the load edge
+    (``load_mid``: the x = nelx edge at z = nelz // 2 instead of z = 0)."""
+
+    nelx: int
+    nely: int
+    nelz: int
+    volfrac: float
+    rmin: float
+    cylinders: List[tuple] = field(default_factory=list)
+    load_mid: bool = False
+    penal: float = 3.0
+
+
+def batched_cantilevers(n: int = 64, seed: int = 0) -> List[DesignSpec]:
+    """The seeded batch: nelx ~ U{24..96}, nely = nelx // 2, nelz ~ U{12..48},
+    volfrac ~ U[0.15, 0.4], rmin ~ U[1.5, 3.5], 0-3 void cylinders of radius
+    U{2..8} with random axis and centre, load on the z = 0 or z = nelz // 2 edge
+    by coin flip."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nelx = int(rng.integers(24, 97))
+        nely = nelx // 2
+        nelz = int(rng.integers(12, 49))
+        dims = (nelx, nely, nelz)
+        cyl = []
+        for _ in range(int(rng.integers(0, 4))):
+            axis = int(rng.integers(0, 3))
+            a, b = [i for i in range(3) if i != axis]
+            cyl.append((axis, int(rng.integers(0, dims[a])), int(rng.integers(0, dims[b])),
+                        int(rng.integers(2, 9))))
+        out.append(DesignSpec(nelx, nely, nelz, float(rng.uniform(0.15, 0.4)), float(rng.uniform(1.5, 3.5)),
+                              cyl, bool(rng.integers(0, 2))))
+    return out
+
+
+def design_problem(spec: DesignSpec):
+    """Masks, total-unit load, fixed DOFs of one design: clamped at x = 0, the
+    -z load on the chosen x = nelx edge; elements at the clamped face and at the
+    loaded nodes are protected solid (optimizer.py:366-390), void wins over
+    solid (:392-399)."""
+    nelx, nely, nelz = spec.nelx, spec.nely, spec.nelz
+    shape = (nely, nelx, nelz)
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    void = np.zeros(shape, bool)
+    for axis, ca, cb, r in spec.cylinders:
+        void |= cylinder_mask_elements(shape, ca, cb, r, axis)
+    F = np.zeros(ndof)
+    iz = nelz // 2 if spec.load_mid else 0
+    for iy in range(nely + 1):
+        F[3 * (iy + (nely + 1) * (nelx + (nelx + 1) * iz)) + 2] = -1.0 / (nely + 1)
+    solid = _elements_at_loaded_nodes(F[None, :], nelx, nely, nelz)
+    solid[:, 0, :] = True
+    solid &= ~void
+    free, _ = build_supports(nelx, nely, nelz, ndof)
+    fixed = np.ones(ndof, np.uint8)
+    fixed[free] = 0
+    return shape, solid, void, F, fixed
+
+
+class BatchRunner:
+    """One ``SimpLoop`` per design on its own stream; ``run(iterations)``
+    advances every design by that many loop bodies with ``workers`` host
+    threads (design i is always driven by thread i % workers)."""
+
+    def __init__(self, specs: List[DesignSpec], precision: str = "mixed", beta: float = 1.0, eta: float = 0.5,
+                 move: float = 0.2, workers: int = 8, solver_options: Optional[dict] = None):
+        self.specs = list(specs)
+        self.workers = max(1, min(int(workers), len(self.specs)))
+        self.streams = [torch.cuda.Stream(device=device()) for _ in self.specs]
+        self.loops: List[SimpLoop] = [None] * len(self.specs)
+        self.ndof = [3 * (s.nelx + 1) * (s.nely + 1) * (s.nelz + 1) for s in self.specs]
+        KE = lk_H8(elem_size=1.0)
+
+        def build(i):
+            spec = self.specs[i]
+            with torch.cuda.stream(self.streams[i]):
+                shape, solid, void, F, fixed = design_problem(spec)
+                loop = SimpLoop(spec.nelx, spec.nely, spec.nelz, spec.volfrac, spec.penal, spec.rmin, KE, F,
+                                fixed, solid, void, projection_eta=eta, move=move, precision=precision,
+                                solver_options=solver_options)
+                loop.set_beta(beta)
+                self.loops[i] = loop
+
+        self._each(build)
+        torch.cuda.synchronize()
+        self.cg_iterations = [0] * len(self.specs)
+        self.compliance = [float("nan")] * len(self.specs)
+
+    def _each(self, fn):
+        """fn(i) for every design, design i on thread i % workers; re-raises."""
+        def worker(w):
+            for i in range(w, len(self.specs), self.workers):
+                fn(i)
+
+        with ThreadPoolExecutor(self.workers) as ex:
+            for f in [ex.submit(worker, w) for w in range(self.workers)]:
+                f.result()
+
+    def run(self, iterations: int) -> dict:
+        """Advance every design; returns wall time, SIMP iterations/s and
+        DOF * CG-iterations/s of the whole batch."""
+        torch.cuda.synchronize()
+        cg0 = list(self.cg_iterations)
+        lock = threading.Lock()
+
+        def advance(i):
+            loop = self.loops[i]
+            with torch.cuda.stream(self.streams[i]):
+                cg = 0
+                st = None
+                for _ in range(iterations):
+                    st = loop.step()
+                    cg += loop.last["cg_iterations"]
+                c = float(st[0]) if st is not None else float("nan")
+            with lock:
+                self.cg_iterations[i] += cg
+                self.compliance[i] = c
+
+        t0 = time.perf_counter()
+        self._each(advance)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        n = len(self.specs)
+        dof_cg = sum(self.ndof[i] * (self.cg_iterations[i] - cg0[i]) for i in range(n))
+        return {"seconds": dt, "designs": n, "iterations": iterations,
+                "simp_iterations_per_s": n * iterations / dt, "dof_cg_iterations_per_s": dof_cg / dt}
+
+    def design(self, i: int) -> torch.Tensor:
+        torch.cuda.synchronize()
+        return self.loops[i].design()
+
+    def close(self):
+        for loop in self.loops:
+            if loop is not None:
+                loop.close()
