@@ -171,6 +171,9 @@ typedef struct tp3d_solver_opts {
   int device_loop;      /* 1: the CG loop runs on the device (one CUDA graph per solve with a
                            conditional WHILE node); 0: the host replays a one-iteration graph and
                            polls the stop flag (profilers see the loop's kernels only then) */
+  int deep_sweeps;      /* smoother degree on levels >= 2; 0: as coarse_sweeps.  Default 4: the
+                           deep levels are small and latency-bound, so more smoothing there costs
+                           little and saves CG iterations (measured on the 128x64x64 cantilever) */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

@@ -52,6 +52,7 @@ class SolverOpts(C.Structure):
         ("galerkin", i32),
         ("coarse_sweeps", i32),
         ("device_loop", i32),
+        ("deep_sweeps", i32),
     ]
 
 

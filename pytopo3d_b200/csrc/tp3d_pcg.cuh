@@ -81,18 +81,27 @@ __global__ void masked_norm_kernel(long long nn, const double* __restrict__ b, c
 
 // u += alpha p; r -= alpha q; partials of ||r||^2 (with fin_count, the last
 // block applies op to st)
+// With fs.x0 set, also the V-cycle's first smoothing step from the new
+// residual (pointwise: x0 = w dinv r, d = x0), as smooth_zero_kernel computes it.
 template <typename T>
 __global__ void cg_update_kernel(long long n, T* u, const T* __restrict__ p, T* r, const T* __restrict__ q,
-                                 PcgState* st, double* partials, int op = 0, unsigned int* fin_count = nullptr) {
+                                 PcgState* st, double* partials, int op = 0, unsigned int* fin_count = nullptr,
+                                 CoarseFirstStep<T> fs = CoarseFirstStep<T>{}) {
   if (*(volatile const int*)&st->done) return;
   __shared__ double red[32];
   const T a = (T)st->alpha;
+  const T w = fs.x0 ? (fs.coef ? (T)fs.coef[0] : fs.omega) : T(0);
   double s = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     u[i] += a * p[i];
     const T ri = r[i] - a * q[i];
     r[i] = ri;
     s += (double)ri * (double)ri;
+    if (fs.x0) {
+      const T v = w * fs.dinv[i] * ri;
+      fs.x0[i] = v;
+      if (fs.d) fs.d[i] = v;
+    }
   }
   s = block_sum(s, red);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;

@@ -580,9 +580,31 @@ struct tp3d_solver {
     return (int)std::max<long long>(1, std::min<long long>(need, (long long)occ * nsm));
   }
 
+  // The first smoothing step of level L from zero, for kernels that compute it
+  // alongside the right-hand side (none when there is no hierarchy).
+  template <typename T>
+  CoarseFirstStep<T> first_step(int L) {
+    CoarseFirstStep<T> fs;
+    if (nlev == 1 || L >= nlev - 1) return fs;
+    auto& lv = levels<T>()[L];
+    const bool cheb = o.smoother != 1;
+    fs.dinv = lv.dinv;
+    fs.coef = cheb ? coef[L] : nullptr;
+    fs.omega = (T)o.omega;
+    fs.x0 = lv.x[0];
+    fs.d = cheb ? lv.d : nullptr;
+    return fs;
+  }
+
   // smoothing degrees of level L (coarse_sweeps > 0 overrides both on levels >= 1)
-  int pre_sweeps(int L) const { return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.pre_sweeps; }
-  int post_sweeps(int L) const { return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.post_sweeps; }
+  int pre_sweeps(int L) const {
+    if (L > 1 && o.deep_sweeps > 0) return o.deep_sweeps;
+    return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.pre_sweeps;
+  }
+  int post_sweeps(int L) const {
+    if (L > 1 && o.deep_sweeps > 0) return o.deep_sweeps;
+    return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.post_sweeps;
+  }
 
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
@@ -873,10 +895,11 @@ struct tp3d_solver {
     io.fin_op = kFinPQ;
     io.fin_count = fin_count;
     int rc = fine<double, kModeCgQ>(io);
-    cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRR, fin_count);
+    const CoarseFirstStep<double> fs0 = first_step<double>(0);
+    cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRR, fin_count, fs0);
     count_launch();
     bool dot_done = false;
-    double* z = vcycle<double>(0, K.r, done, &rc, false, kFinRZ, &dot_done);
+    double* z = vcycle<double>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZ, &dot_done);
     if (!dot_done) {
       dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZ, fin_count);
       count_launch();
@@ -997,7 +1020,9 @@ struct tp3d_solver {
     io.fin_op = kFinPQMixed;
     io.fin_count = fin_count;
     int rc = fine<float, kModeCgQ>(io);
-    cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRRMixed, fin_count);
+    const CoarseFirstStep<float> fs0 = first_step<float>(0);
+    cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRRMixed, fin_count,
+                                                fs0);
     count_launch();
     // reliable update (each kernel is also gated on state->update itself)
     rc |= update_branch([&]() {
@@ -1014,11 +1039,16 @@ struct tp3d_solver {
                                              fin_count);
       count_launch();
       demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K.r, state, 0); count_launch();
+      if (fs0.x0) {  // the first smoothing step again, from the replaced residual
+        smooth_zero_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, fs0.dinv, fs0.omega, fs0.coef, fs0.x0, fs0.d,
+                                                      done);
+        count_launch();
+      }
       clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
       return brc;
     });
     bool dot_done = false;
-    float* z = vcycle<float>(0, K.r, done, &rc, false, kFinRZMixed, &dot_done);
+    float* z = vcycle<float>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZMixed, &dot_done);
     if (!dot_done) {
       dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZMixed, fin_count);
       count_launch();
@@ -1195,6 +1225,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->galerkin = 0;
   o->coarse_sweeps = 2;
   o->device_loop = 1;
+  o->deep_sweeps = 4;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1215,6 +1246,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       !(o.cheb_ratio > 1.0) || o.power_iterations < 2 || !(o.reliable_delta > 0.0 && o.reliable_delta < 1.0))
     return fail(TP3D_ERR_ARG, "invalid solver options");
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
+  if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
   if (o.smoother != 1 && o.pre_sweeps != o.post_sweeps)
     return fail(TP3D_ERR_ARG, "pre_sweeps and post_sweeps must be equal: the Chebyshev V-cycle preconditions CG and "
                               "must stay symmetric");
