@@ -88,6 +88,7 @@ template <int Z>
 __global__ void __launch_bounds__(kFilterThreads) rowsum_kernel(Grid g, FilterCols fc, double* Hs) {
   extern __shared__ double s[];
   const FilterTile t = filter_tile_at(g, blockIdx.x);
+  filter_cols_to_smem<Z>(fc, s);
   filter_stage<Z>(g, t, s, [](long long, int, int, int) { return 1.0; });
   __syncthreads();
   filter_apply<Z>(g, fc, t, s, [&](long long e, int, int, int, double v) { Hs[e] = (v == 0.0) ? 1.0 : v; });
@@ -101,6 +102,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                    double* rf, double* rp, double* dp) {
   extern __shared__ double s[];
   const FilterTile t = filter_tile_at(g, blockIdx.x);
+  filter_cols_to_smem<Z>(fc, s);
   filter_stage<Z>(g, t, s, [&](long long e, int, int, int) { return __ldg(&x[e]); });
   __syncthreads();
   filter_apply<Z>(g, fc, t, s, [&](long long e, int, int, int, double v) {
@@ -124,6 +126,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                      const double* __restrict__ Hs, double* out) {
   extern __shared__ double s[];
   const FilterTile t = filter_tile_at(g, blockIdx.x);
+  filter_cols_to_smem<Z>(fc, s);
   filter_stage<Z>(g, t, s, [&](long long e, int, int, int) {
     const double gd = dp ? __ldg(&gin[e]) * __ldg(&dp[e]) : __ldg(&gin[e]);
     return gd / __ldg(&Hs[e]);
@@ -152,7 +155,7 @@ int check_grid(int nx, int ny, int nz) {
 
 template <class K>
 int launch_filter(K kernel, const Grid& g, int Z, cudaStream_t st) {
-  const size_t smem = (size_t)filter_smem_elems(Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(Z);
   TP3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   (void)st;
   return TP3D_OK;
@@ -170,7 +173,7 @@ extern "C" int tp3d_filter_rowsum(int nelx, int nely, int nelz, double rmin, dou
   if (int rc = filter_cols_for(rmin, &fc)) return rc;
   const Grid g{nelx, nely, nelz};
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t smem = (size_t)filter_smem_elems(fc.Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(fc.Z);
   TP3D_DISPATCH_Z(fc.Z, {
     if (int rc = launch_filter(rowsum_kernel<ZC>, g, ZC, st)) return rc;
     rowsum_kernel<ZC><<<(unsigned)filter_ntiles(g), kFilterThreads, smem, st>>>(g, fc, Hs);
@@ -198,7 +201,7 @@ extern "C" int tp3d_filter_project(int nelx, int nely, int nelz, double rmin, co
   if (int rc = filter_cols_for(rmin, &fc)) return rc;
   const Grid g{nelx, nely, nelz};
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t smem = (size_t)filter_smem_elems(fc.Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(fc.Z);
   const Projection pr(beta, eta);
   TP3D_DISPATCH_Z(fc.Z, {
     if (int rc = launch_filter(project_kernel<ZC>, g, ZC, st)) return rc;
@@ -218,7 +221,7 @@ extern "C" int tp3d_filter_transpose(int nelx, int nely, int nelz, double rmin, 
   if (int rc = filter_cols_for(rmin, &fc)) return rc;
   const Grid g{nelx, nely, nelz};
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t smem = (size_t)filter_smem_elems(fc.Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(fc.Z);
   TP3D_DISPATCH_Z(fc.Z, {
     if (int rc = launch_filter(transpose_kernel<ZC>, g, ZC, st)) return rc;
     transpose_kernel<ZC><<<(unsigned)filter_ntiles(g), kFilterThreads, smem, st>>>(g, fc, gin, dproj, Hs, out);

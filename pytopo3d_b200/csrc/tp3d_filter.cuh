@@ -34,6 +34,26 @@ __host__ __device__ inline int filter_smem_elems(int Z) {
   return (kFilterTY + 2 * Z) * (kFilterTX + 2 * Z) * (kFilterKZ + 2 * Z);
 }
 
+// Columns of a radius with max offset Z: at most (2Z+1)^2.  Kernels copy the
+// column table (weights, then offsets) into shared memory after the staged
+// tile, so the stencil loop reads it with broadcast shared loads.
+__host__ __device__ inline int filter_max_cols(int Z) { return (2 * Z + 1) * (2 * Z + 1); }
+__host__ __device__ inline size_t filter_smem_bytes(int Z) {
+  return (size_t)filter_smem_elems(Z) * sizeof(double) +
+         (size_t)filter_max_cols(Z) * ((2 * Z + 1) * sizeof(double) + sizeof(int2));
+}
+
+// Copy fc's table into the shared table area of `s` (call before a barrier
+// that precedes the first filter_apply).
+template <int Z>
+__device__ __forceinline__ void filter_cols_to_smem(const FilterCols& fc, double* s) {
+  constexpr int W = 2 * Z + 1;
+  double* sw = s + filter_smem_elems(Z);
+  int2* sd = reinterpret_cast<int2*>(sw + filter_max_cols(Z) * W);
+  for (int i = threadIdx.x; i < fc.ncols * W; i += blockDim.x) sw[i] = __ldg(&fc.w[i]);
+  for (int i = threadIdx.x; i < fc.ncols; i += blockDim.x) sd[i] = fc.dxy[i];
+}
+
 struct FilterTile {
   int x0, y0, z0;
 };
@@ -77,15 +97,17 @@ __device__ __forceinline__ void filter_apply(const Grid& g, const FilterCols& fc
   constexpr int SY = kFilterTY + 2 * Z, SX = kFilterTX + 2 * Z;
   constexpr int W = 2 * Z + 1;
   const int ly = threadIdx.x % kFilterTY, lx = threadIdx.x / kFilterTY;
+  const double* sw = s + filter_smem_elems(Z);  // table copied by filter_cols_to_smem
+  const int2* sd = reinterpret_cast<const int2*>(sw + filter_max_cols(Z) * W);
   double acc[kFilterKZ];
 #pragma unroll
   for (int k = 0; k < kFilterKZ; ++k) acc[k] = 0.0;
   for (int c = 0; c < fc.ncols; ++c) {
-    const int2 d = __ldg(&fc.dxy[c]);
-    const double* wc = fc.w + (size_t)c * W;
+    const int2 d = sd[c];
+    const double* wc = sw + c * W;
     double wv[W];
 #pragma unroll
-    for (int j = 0; j < W; ++j) wv[j] = __ldg(&wc[j]);
+    for (int j = 0; j < W; ++j) wv[j] = wc[j];
     const double* col = s + (size_t)(lx + Z + d.x) * SY + (ly + Z + d.y);
     double v[kFilterKZ + 2 * Z];
 #pragma unroll

@@ -101,6 +101,7 @@ __device__ bool oc_volume(const OcArgs& a, double lam, double* part, double* s, 
 template <int Z>
 __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   extern __shared__ double s[];
+  filter_cols_to_smem<Z>(a.fc, s);  // read back after the first barrier
   __shared__ double red[32];
   const long long ntiles = filter_ntiles(a.g);
   const long long nele = a.g.nele();
@@ -290,7 +291,7 @@ extern "C" int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const d
   int dev = 0, nsm = 0;
   TP3D_CHECK(cudaGetDevice(&dev));
   TP3D_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const size_t smem = (size_t)filter_smem_elems(fc.Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(fc.Z);
   const long long ntiles = filter_ntiles(g);
   TP3D_DISPATCH_Z(fc.Z, {
     auto kern = oc_kernel<ZC>;
@@ -462,7 +463,7 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
   int dev = 0, nsm = 0;
   TP3D_CHECK(cudaGetDevice(&dev));
   TP3D_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const size_t smem = (size_t)filter_smem_elems(Z) * sizeof(double);
+  const size_t smem = filter_smem_bytes(Z);
   const long long ntiles = filter_ntiles(g);
   TP3D_DISPATCH_Z(Z, {
     auto kern = oc_kernel<ZC>;

@@ -230,6 +230,9 @@ struct tp3d_solver {
   bool loop_ok = true, in_loop_capture = false, branch_ok = true;
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
+  cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
+  cudaEvent_t ev_side_in = nullptr, ev_side_out = nullptr;
+  int* cstatus_host = nullptr;        // pinned copy of the inverse's status
   unsigned int* loop_passes = nullptr;
   unsigned int* loop_pass_host = nullptr;
   PcgState* state = nullptr;
@@ -269,6 +272,10 @@ struct tp3d_solver {
     if (state_host) cudaFreeHost(state_host);
     if (loop_pass_host) cudaFreeHost(loop_pass_host);
     if (st_branch) cudaStreamDestroy(st_branch);
+    if (st_side) cudaStreamDestroy(st_side);
+    if (ev_side_in) cudaEventDestroy(ev_side_in);
+    if (ev_side_out) cudaEventDestroy(ev_side_out);
+    if (cstatus_host) cudaFreeHost(cstatus_host);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     if (st) cudaStreamDestroy(st);
@@ -1316,7 +1323,11 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   if (s->fin_count) cudaMemset(s->fin_count, 0, sizeof(unsigned int));
   s->loop_passes = s->alloc<unsigned int>(1);
   if (cudaMallocHost(&s->loop_pass_host, sizeof(unsigned int)) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s->st_branch, cudaStreamNonBlocking) != cudaSuccess)
+      cudaStreamCreateWithFlags(&s->st_branch, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_side_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_side_out, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&s->cstatus_host, sizeof(int)) != cudaSuccess)
     return fail(TP3D_ERR_CUDA, "solver setup failed");
   s->state = s->alloc<PcgState>(1);
   unsigned int* cnt = s->alloc<unsigned int>(4);
@@ -1528,13 +1539,68 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // FP64 form, or the mixed form's fallback
     TP3D_CHECK_LAUNCH();
   }
+  // The coarsest inverse (one block) runs on a side stream while the power
+  // iterations below use the rest of the GPU; its status is read after both.
+  auto coarsest_gj = [&](cudaStream_t cs, double shift) -> int {
+    const int L = s->nlev - 1;
+    const int n = s->cn;
+    TP3D_CHECK(cudaMemsetAsync(s->cdense, 0, (size_t)n * n * sizeof(double), cs));
+    dense_from_stencil_kernel<<<s->grid_blocks(s->grids[L].nnode()), 256, 0, cs>>>(s->grids[L], s->A64[L], s->fix[L],
+                                                                                    s->cdense);
+    count_launch();
+    if (shift > 0.0) {
+      dense_shift_kernel<<<s->grid_blocks(n), 256, 0, cs>>>(n, s->cdense, shift);
+      count_launch();
+    }
+    if (n <= kGjRegMaxN) {
+      dense_gj_inverse_reg_kernel<<<1, 512, 0, cs>>>(n, s->cdense, s->cinv64, s->cstatus);
+      count_launch();
+    } else {
+      const size_t smem = 2 * (size_t)n * sizeof(double);
+      if (smem > 48 * 1024)
+        TP3D_CHECK(cudaFuncSetAttribute(dense_gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+      dense_gj_inverse_kernel<<<1, 1024, smem, cs>>>(n, s->cdense, s->cinv64, 0, s->cstatus);
+      count_launch();
+    }
+    if (mixed) {
+      convert_kernel<double, float><<<s->grid_blocks((long long)n * n), 256, 0, cs>>>((long long)n * n, s->cinv64,
+                                                                                      s->cinv32);
+      count_launch();
+    }
+    TP3D_CHECK(cudaMemcpyAsync(s->cstatus_host, s->cstatus, sizeof(int), cudaMemcpyDeviceToHost, cs));
+    TP3D_CHECK_LAUNCH();
+    return TP3D_OK;
+  };
   if (s->nlev > 1) {
+    TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
+    TP3D_CHECK(cudaStreamWaitEvent(s->st_side, s->ev_side_in, 0));
+    if (int rc = coarsest_gj(s->st_side, 0.0)) return rc;
+    TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
+  }
+  if (s->o.smoother != 1)
+    if (int rc = mixed ? estimate_spectra<float>(s) : estimate_spectra<double>(s)) return rc;
+  if (s->nlev > 1) {
+    TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
+    TP3D_CHECK(cudaEventSynchronize(s->ev_side_out));
+  }
+  if (s->nlev > 1 && *s->cstatus_host != 0) {
     const int L = s->nlev - 1;
     const int n = s->cn;
     double shift = 0.0;
     s->coarse_fallback = false;
     int status = 1;
+    // the unshifted attempt failed: retry with shifts on the solver's stream
     for (int attempt = 0; attempt < 3 && status != 0; ++attempt) {
+      {
+        std::vector<double> h((size_t)243 * s->grids[L].nnode());
+        cudaMemcpy(h.data(), s->A64[L], h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        const long long nnL = s->grids[L].nnode();
+        double dsum = 0.0;
+        for (long long i = 0; i < nnL; ++i)
+          for (int c = 0; c < 3; ++c) dsum += std::fabs(h[(size_t)stencil_k(13, c, c) * nnL + i]);
+        shift = (shift == 0.0 ? 1e-12 : shift * 1e3) * std::max(dsum / n, 1e-300);
+      }
       TP3D_CHECK(cudaMemsetAsync(s->cdense, 0, (size_t)n * n * sizeof(double), st));
       dense_from_stencil_kernel<<<s->grid_blocks(s->grids[L].nnode()), 256, 0, st>>>(s->grids[L], s->A64[L],
                                                                                       s->fix[L], s->cdense);
@@ -1557,16 +1623,6 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       TP3D_CHECK_LAUNCH();
       TP3D_CHECK(cudaMemcpyAsync(&status, s->cstatus, sizeof(int), cudaMemcpyDeviceToHost, st));
       TP3D_CHECK(cudaStreamSynchronize(st));
-      if (status != 0) {
-        // not positive definite in floating point: shift relative to the mean diagonal and retry
-        std::vector<double> h((size_t)243 * s->grids[L].nnode());
-        cudaMemcpy(h.data(), s->A64[L], h.size() * sizeof(double), cudaMemcpyDeviceToHost);
-        const long long nnL = s->grids[L].nnode();
-        double dsum = 0.0;
-        for (long long i = 0; i < nnL; ++i)
-          for (int c = 0; c < 3; ++c) dsum += std::fabs(h[(size_t)stencil_k(13, c, c) * nnL + i]);
-        shift = (shift == 0.0 ? 1e-12 : shift * 1e3) * std::max(dsum / n, 1e-300);
-      }
     }
     if (status != 0) {  // fall back to the inverse diagonal of the coarsest operator
       s->coarse_fallback = true;
@@ -1582,9 +1638,9 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
                                                                                       s->cinv32);
       count_launch();
     }
+  } else if (s->nlev > 1) {
+    s->coarse_fallback = false;
   }
-  if (s->o.smoother != 1)
-    if (int rc = mixed ? estimate_spectra<float>(s) : estimate_spectra<double>(s)) return rc;
   TP3D_CHECK_LAUNCH();
   s->have_density = true;
   return s->leave();
