@@ -59,8 +59,38 @@ __device__ __forceinline__ void build_l1_rows(const Grid& gf, const Grid& gc, co
   }
 }
 
+// The rows this thread built (node n, row component c, z-offset dzr), also
+// in the apply layout of stencil_pack_kernel: fixed rows / columns and
+// neighbours past the grid set to zero.
+template <typename TP>
+__device__ __forceinline__ void store_packed_rows(const Grid& g, const uint8_t* __restrict__ fix, long long n, int ix,
+                                                  int iy, int iz, int c, int dzr, const double (&acc)[9][3],
+                                                  TP* P) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const long long ndof = 3 * g.nnode();
+  const bool fi = (fix[n] >> c) & 1;
+  const int z = iz + dzr;
+#pragma unroll
+  for (int jx = -1; jx <= 1; ++jx)
+#pragma unroll
+    for (int jy = -1; jy <= 1; ++jy) {
+      const int x = ix + jx, y = iy + jy;
+      const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
+      const int fm = in ? fix[g.nidx(x, y, z)] : 7;
+      const int jr = jrel_of(jx, jy, dzr);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double v = (fi || ((fm >> d) & 1)) ? 0.0 : acc[(jx + 1) * 3 + (jy + 1)][d];
+        P[(long long)(jr * 3 + d) * ndof + 3 * n + c] = (TP)v;
+      }
+    }
+}
+
+// With P given, also writes the apply layout (see store_packed_rows).
+template <typename TP>
 __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Grid gc, const double* __restrict__ E,
-                                                                     const double* __restrict__ KE1, double* A) {
+                                                                     const double* __restrict__ KE1, double* A,
+                                                                     const uint8_t* __restrict__ fixc, TP* P) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = gc.nnode();
@@ -85,6 +115,7 @@ __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Gr
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
+  if (P) store_packed_rows<TP>(gc, fixc, n, Ix, Iy, Iz, c, dzr, acc, P);
 }
 
 // ---- stencil Galerkin product A_c = P^T A_f P ----
@@ -246,8 +277,10 @@ __global__ void __launch_bounds__(576) elem_coarsen_kernel(Grid gf, Grid gc, con
 // Stencil (27-point 3x3 blocks, layout of stencil_k) of level g assembled
 // from its element matrices.  Threads as in the other builders: a warp per 32
 // nodes for one (row component c, z-offset dzr).
+template <typename TP>
 __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid g, const double* __restrict__ Ke,
-                                                                           double* A) {
+                                                                           double* A, const uint8_t* __restrict__ fix,
+                                                                           TP* P) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = g.nnode();
@@ -294,6 +327,7 @@ __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid 
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
+  if (P) store_packed_rows<TP>(g, fix, n, ix, iy, iz, c, dzr, acc, P);
 }
 
 // ---- coarse fixed-DOF masks ----

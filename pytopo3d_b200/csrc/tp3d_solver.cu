@@ -1512,20 +1512,38 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       if (int rc = s->choose_fine_form<float>()) return rc;
     s->fine_chosen = true;
   }
+  // Element matrices of levels >= 2 depend only on the fine moduli: they are
+  // built on the side stream while level 1 is built here.
+  const bool elem_chain = s->o.galerkin == 0 && s->nlev > 2;
+  if (elem_chain) {
+    TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
+    TP3D_CHECK(cudaStreamWaitEvent(s->st_side, s->ev_side_in, 0));
+    for (int L = 2; L < s->nlev; ++L) {
+      const unsigned ne = (unsigned)s->grids[L].nele();
+      if (L == 2) elem2_from_fine_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[0], s->grids[2], s->E64, s->KE2, s->Kel[2]);
+      else elem_coarsen_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[L - 1], s->grids[L], s->Kel[L - 1], s->Kel[L]);
+      count_launch();
+    }
+    TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
+  }
   for (int L = 1; L < s->nlev; ++L) {
     const Grid& gf = s->grids[L - 1];
     const Grid& gc = s->grids[L];
     const unsigned nb = (unsigned)((gc.nnode() + 31) / 32);
+    if (L == 2 && elem_chain) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
+    // the builders also write the packed (apply) layout of the solve's precision
+    float* P32 = mixed ? s->L32[L].A : nullptr;
+    double* P64 = mixed ? nullptr : s->L64[L].A;
+    bool packed = true;
     if (L == 1) {
-      build_level1_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1]);
+      if (mixed) build_level1_kernel<float><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P32);
+      else build_level1_kernel<double><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P64);
     } else if (s->o.galerkin == 0) {
-      const unsigned ne = (unsigned)gc.nele();
-      if (L == 2) elem2_from_fine_kernel<<<ne, 576, 0, st>>>(s->grids[0], gc, s->E64, s->KE2, s->Kel[2]);
-      else elem_coarsen_kernel<<<ne, 576, 0, st>>>(gf, gc, s->Kel[L - 1], s->Kel[L]);
-      count_launch();
-      stencil_from_elems_kernel<<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L]);
+      if (mixed) stencil_from_elems_kernel<float><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P32);
+      else stencil_from_elems_kernel<double><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P64);
     } else {
       rap_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->A64[L - 1], s->A64[L]);
+      packed = false;
     }
     count_launch();
     const long long nn = gc.nnode();
@@ -1534,9 +1552,11 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     if (mixed) {
       convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
       count_launch();
-      s->pack_level<float>(L, s->L32[L].A);
+      if (!packed) s->pack_level<float>(L, s->L32[L].A);
+      if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // the mixed form's FP64 fallback
+    } else if (!packed) {
+      s->pack_level<double>(L, s->L64[L].A);
     }
-    if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // FP64 form, or the mixed form's fallback
     TP3D_CHECK_LAUNCH();
   }
   // The coarsest inverse (one block) runs on a side stream while the power
