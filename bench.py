@@ -322,19 +322,23 @@ def main():
     steps = main_r["steps"]
     rate = job_rate(steps, main_r["ms"] / 1e3, world)
 
-    # end-to-end through the public API with host buffers (pinned H2D of x, D2H of x_new + c)
-    x_host = loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
-    for _ in range(2):
-        x_host, _ = loop.step_host(x_host)
+    # end-to-end through the public API with host buffers (pinned H2D of x, D2H of x_new + c):
+    # a fresh loop from the same start, the same warm-up and the same number of
+    # steps as the device-timed run, so both follow the same trajectory
+    e2e_loop = make_loop(args.precision)
+    x_host = e2e_loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
+    for _ in range(W):
+        x_host, _ = e2e_loop.step_host(x_host)
     barrier(dist)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e_steps = max(3, args.steps // 2)
+    e_steps = steps
     for _ in range(e_steps):
-        x_host, c_host = loop.step_host(x_host)
+        x_host, c_host = e2e_loop.step_host(x_host)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     e2e_rate = job_rate(e_steps, e2e_s, world)
+    e2e_loop.close()
 
     # roofline of the dominant kernel (fine-level operator apply)
     peak, peak_kind = peaks()
