@@ -344,6 +344,7 @@ def top3d(
 
     total_loop = 0
     c = float("nan")
+    snap = torch.empty(nelx * nely * nelz, dtype=torch.float64, pin_memory=True) if save_history else None
     stage_summaries = []
     for beta in beta_schedule:
         logger.info("Starting projection stage: beta=%g", beta)
@@ -366,7 +367,10 @@ def top3d(
             stage_loop += 1
             total_loop += 1
             t0 = time.time()
-            rho_used = S.rho_p.clone() if save_history else None
+            if save_history:
+                # the design this iteration solves on, copied to pinned host memory
+                # while the iteration runs (read only if the iteration is recorded)
+                snap.copy_(S.rho_p, non_blocking=True)
             cg_iters = S.sensitivities(S.rho_p, S.dproj)
             stats = oc_update_flat(H, x, S.dc_dx, S.dv_dx, Hs, solid, void, move, target_free_volume, beta,
                                    projection_eta, S.x_new, S.rho_new, S.ws)
@@ -383,7 +387,7 @@ def top3d(
                                    lam=float(host[1])))
             if save_history and ((total_loop - 1) % history_frequency == 0 or change <= tolx
                                  or stage_loop == maxloop):
-                history["density_history"].append(from_flat(rho_used, expected_shape).cpu().numpy())
+                history["density_history"].append(snap.numpy().reshape(nelz, nelx, nely).transpose(2, 1, 0).copy())
                 history["iteration_history"].append(total_loop - 1)
                 history["compliance_history"].append(c)
                 history["beta_history"].append(beta)
