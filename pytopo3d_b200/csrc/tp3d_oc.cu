@@ -93,7 +93,7 @@ __device__ bool oc_volume(const OcArgs& a, double lam, double* part, double* s, 
   }
   vpart = block_sum(vpart, red);
   if (threadIdx.x == 0) part[blockIdx.x] = vpart;
-  if (!grid_sync(a.bar)) return false;
+  if (!grid_sync_flip(a.bar.count, a.bar.err)) return false;
   *vol = sum_partials(part, gridDim.x, red);
   return true;
 }
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   }
   m = block_max(m, red);
   if (threadIdx.x == 0) a.partC[blockIdx.x] = m;
-  if (!grid_sync(a.bar)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
   double scale = 0.0;
   {
     double t = 0.0;
@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
     else q = sqrt(scale > 0.0 ? a.ratio[e] / scale : 1.0);
     a.ratio[e] = q;
   }
-  if (!grid_sync(a.bar)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
 
   // ---- bisection (oc_update.py:70-122) ----
   // The reference starts from [0, 1e12]; while the projected volume stays at or
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   }
   cmax = block_max(cmax, red);
   if (threadIdx.x == 0) a.partC[blockIdx.x] = cmax;
-  if (!grid_sync(a.bar)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
   for (long long t = blockIdx.x; t < ntiles; t += nblk) {
     const FilterTile tile = filter_tile_at(a.g, t);
     __syncthreads();
