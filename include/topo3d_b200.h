@@ -174,6 +174,10 @@ typedef struct tp3d_solver_opts {
   int deep_sweeps;      /* smoother degree on levels >= 2; 0: as coarse_sweeps.  Default 4: the
                            deep levels are small and latency-bound, so more smoothing there costs
                            little and saves CG iterations (measured on the 128x64x64 cantilever) */
+  int pdl;              /* programmatic dependent launch in the CG loop (each kernel's launch overlaps
+                           the tail of the one before it), a mask: 1 the coarse levels' kernels,
+                           2 the fine operator and fine-level vector kernels, 3 both, 0 plain stream
+                           order.  Turned off by itself when a CUDA graph cannot be built with it. */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -216,7 +220,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * FP64-fallback flag (mixed), fine form of the FP64 operator and of the FP32 operator
  * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent), first level of the fused
  * coarse cycle (0 none), 1 when the CG loop runs on the device (one graph launch per
- * solve) rather than host-polled.  Returns the count written. */
+ * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none).
+ * Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

@@ -53,6 +53,7 @@ class SolverOpts(C.Structure):
         ("coarse_sweeps", i32),
         ("device_loop", i32),
         ("deep_sweeps", i32),
+        ("pdl", i32),
     ]
 
 

@@ -170,6 +170,52 @@ __device__ __forceinline__ bool grid_sync_flip(unsigned int* word, int* err) {
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? TP3D_OK : TP3D_ERR_CUDA; }
 
+// Programmatic dependent launch.  The solver loop's kernels begin with
+// pdl_entry(): wait until the kernel before this one in the stream has
+// completed and its writes are visible (every global access of the kernel
+// comes after this), then let the next kernel's blocks be scheduled as this
+// grid's last blocks run, so that its launch latency overlaps this kernel's
+// tail.  A kernel launched without the programmatic-serialization attribute
+// passes the wait at once.  Kernels with a grid barrier never use it.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Kernel launch, with the programmatic-serialization attribute when pdl is
+// set (the kernel must begin with pdl_entry()).
+template <typename... P, typename... A>
+inline cudaError_t launch_kernel(bool pdl, void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
+                                 cudaStream_t st, A&&... args) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<A&&>(args)...);
+}
+
+// The same for a kernel given as a function pointer and an argument array.
+inline cudaError_t launch_kernel_c(bool pdl, const void* kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                   void** args) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelExC(&cfg, kern, args);
+}
+
 // Process-wide count of kernel launches issued by this library (graph
 // replays add the graph's kernel-node count).
 void add_launches(long long n);

@@ -97,6 +97,7 @@ __device__ __forceinline__ T ke_coef(const KEP<T>& ke, const T (&kc)[kKEClasses]
 
 template <typename T, class ESrc, int TY, int NZT, bool CLS>
 __global__ void __launch_bounds__(256, 2) fine_apply_kernel(const __grid_constant__ FineParams<T, ESrc> p) {
+  pdl_entry();
   if (op_skip(p.io)) return;
   using FT = FineTile<TY>;
   constexpr int PY = FT::PY, PP = FT::PP, EY = FT::EY, EP = FT::EP;

@@ -88,12 +88,12 @@ int wht_occupancy(int v) {
 }
 
 template <typename T, class ESrc>
-int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st) {
+int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st, bool pdl) {
   if (v < 0 || v >= kWhtVariants || !wht_prepare<T, ESrc>(v)) return TP3D_ERR_ARG;
   const int nthr = WhtShapes<T>::nthr[v];
   void* args[] = {(void*)&p};
-  const cudaError_t e = cudaLaunchKernel(wht_fn<T, ESrc>(mode, v), grid, dim3(nthr), args,
-                                         wht_smem_bytes<T>(nthr), st);
+  const cudaError_t e = launch_kernel_c(pdl, wht_fn<T, ESrc>(mode, v), grid, dim3(nthr), wht_smem_bytes<T>(nthr), st,
+                                        args);
   return e == cudaSuccess ? TP3D_OK : TP3D_ERR_CUDA;
 }
 
@@ -182,7 +182,7 @@ WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
 #define TP3D_WHT_INSTANTIATE(T, ESrc)                                                     \
   template int wht_variant_threads<T, ESrc>(int);                                        \
   template int wht_occupancy<T, ESrc>(int);                                              \
-  template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t); \
+  template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t, bool); \
   template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);
 TP3D_WHT_INSTANTIATE(double, EFromF64)
 TP3D_WHT_INSTANTIATE(float, EFromF32)

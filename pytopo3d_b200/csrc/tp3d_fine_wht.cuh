@@ -57,6 +57,7 @@ __host__ __device__ constexpr size_t wht_smem_bytes(int nthr) {
 
 template <typename T, class ESrc, int MODE, int NTHR, int MINB>
 __global__ void __launch_bounds__(NTHR, MINB) wht_apply_kernel(const __grid_constant__ WhtParams<T, ESrc> p) {
+  pdl_entry();
   if (op_skip(p.io)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);  // [3][NTHR] masked u of each thread's node
@@ -261,7 +262,7 @@ int wht_variant_threads(int v);
 template <typename T, class ESrc>
 int wht_occupancy(int v);
 template <typename T, class ESrc>
-int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st);
+int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st, bool pdl = false);
 
 // Walsh-Hadamard blocks of KE (see the top of this file); false when KE is not
 // block diagonal in that basis to 1e-12 of its largest entry, or the

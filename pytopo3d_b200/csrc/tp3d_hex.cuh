@@ -269,6 +269,7 @@ __device__ __forceinline__ T stencil_row(const Grid& g, const T* __restrict__ S,
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T> p) {
+  pdl_entry();
   if (op_skip(p.io)) return;
   __shared__ double red[32];
   const Grid g = p.g;
@@ -307,6 +308,7 @@ __global__ void stencil_diag_inv_kernel(Grid g, const double* __restrict__ A, co
 template <typename T>
 __global__ void smooth_zero_kernel(long long ndof, const T* __restrict__ b, const T* __restrict__ dinv, T omega,
                                    const double* coef, T* x, T* d, const int* done) {
+  pdl_entry();
   if (done && *(volatile const int*)done) return;
   const T w = coef ? (T)coef[0] : omega;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x) {
@@ -382,6 +384,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T* __restrict__ rf,
                                                        const uint8_t* __restrict__ fixc, T* bc, const int* done,
                                                        CoarseFirstStep<T> fs) {
+  pdl_entry();
   if (done && *(volatile const int*)done) return;
   const int CY = gc.ny + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -443,6 +446,7 @@ __device__ __forceinline__ void prolong_node(const Grid& gf, const Grid& gc, con
 template <typename T>
 __global__ void __launch_bounds__(256) prolong_add_kernel(Grid gf, Grid gc, const T* __restrict__ xc,
                                                           const uint8_t* __restrict__ fixf, T* xf, const int* done) {
+  pdl_entry();
   if (done && *(volatile const int*)done) return;
   const int FY = gf.ny + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -528,6 +528,7 @@ __global__ void __launch_bounds__(512, 1) dense_gj_inverse_reg_kernel(int n, con
 
 template <typename T>
 __global__ void dense_matvec_kernel(int n, const T* __restrict__ Inv, const T* __restrict__ b, T* x, const int* done) {
+  pdl_entry();
   if (done && *(volatile const int*)done) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;

@@ -11,6 +11,7 @@ namespace tp3d {
 
 __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgState* st, int op, double rtol2,
                                 double* out) {
+  pdl_entry();
   __shared__ double red[32];
   if (finalize_skipped(st, op)) return;
   const double s = sum_partials(partials, n, red);
@@ -18,7 +19,10 @@ __global__ void finalize_kernel(const double* __restrict__ partials, int n, PcgS
   finalize_apply(s, st, op, rtol2, out);
 }
 
-__global__ void clear_update_kernel(PcgState* st) { st->update = 0; }
+__global__ void clear_update_kernel(PcgState* st) {
+  pdl_entry();
+  st->update = 0;
+}
 
 // Linear extrapolation of successive solutions as the next initial guess:
 // U <- 2 U - U_prev and U_prev <- U (old), or only U_prev <- U when there is no
@@ -54,6 +58,7 @@ template <typename T>
 __global__ void dot_kernel(long long n, const T* __restrict__ a, const T* __restrict__ b, double* partials,
                            const int* done, const int* gate, PcgState* st = nullptr, int op = 0,
                            unsigned int* fin_count = nullptr) {
+  pdl_entry();
   if ((done && *(volatile const int*)done) || (gate && *(volatile const int*)gate == 0)) return;
   __shared__ double red[32];
   double s = 0.0;
@@ -67,6 +72,7 @@ __global__ void dot_kernel(long long n, const T* __restrict__ a, const T* __rest
 // ||b||^2 over free DOFs
 __global__ void masked_norm_kernel(long long nn, const double* __restrict__ b, const uint8_t* __restrict__ fix,
                                    double* partials) {
+  pdl_entry();
   __shared__ double red[32];
   double s = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
@@ -87,6 +93,7 @@ template <typename T>
 __global__ void cg_update_kernel(long long n, T* u, const T* __restrict__ p, T* r, const T* __restrict__ q,
                                  PcgState* st, double* partials, int op = 0, unsigned int* fin_count = nullptr,
                                  CoarseFirstStep<T> fs = CoarseFirstStep<T>{}) {
+  pdl_entry();
   if (*(volatile const int*)&st->done) return;
   __shared__ double red[32];
   const T a = (T)st->alpha;
@@ -111,6 +118,7 @@ __global__ void cg_update_kernel(long long n, T* u, const T* __restrict__ p, T* 
 // p = z + beta p (or p = z)
 template <typename T>
 __global__ void cg_p_kernel(long long n, const T* __restrict__ z, T* p, const PcgState* st, int init) {
+  pdl_entry();
   if (!init && *(volatile const int*)&st->done) return;
   const T b = init ? T(0) : (T)st->beta;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -119,6 +127,7 @@ __global__ void cg_p_kernel(long long n, const T* __restrict__ z, T* p, const Pc
 
 // Reliable update: u64 += x32, x32 = 0 (only when st->update, or always with force).
 __global__ void flush_kernel(long long n, double* u, float* x, const PcgState* st, int force) {
+  pdl_entry();
   if (!force && (*(volatile const int*)&st->done || *(volatile const int*)&st->update == 0)) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     u[i] += (double)x[i];
@@ -128,6 +137,7 @@ __global__ void flush_kernel(long long n, double* u, float* x, const PcgState* s
 
 // r32 = float(r64), gated like the reliable update
 __global__ void demote_kernel(long long n, const double* __restrict__ r, float* out, const PcgState* st, int force) {
+  pdl_entry();
   if (!force && (*(volatile const int*)&st->done || *(volatile const int*)&st->update == 0)) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = (float)r[i];

@@ -40,6 +40,7 @@ inline void count_launch() {
 }
 
 constexpr int kMaxPartials = 1 << 16;
+constexpr int kPdlCoarse = 1, kPdlFine = 2;  // tp3d_solver_opts::pdl bits
 
 template <typename T>
 struct LevelVec {
@@ -68,12 +69,13 @@ struct Tile {
 
 // Launch / occupancy of the fine operator for a compile-time tile height.
 template <typename T, class ESrc, bool CLS>
-int fine_launch_t(const FineParams<T, ESrc>& p, int TY, dim3 grid, int threads, cudaStream_t st) {
+int fine_launch_t(const FineParams<T, ESrc>& p, int TY, dim3 grid, int threads, cudaStream_t st, bool pdl) {
   constexpr int NZT = sizeof(T) == 4 ? 2 : 1;
   switch (TY) {
 #define TP3D_FINE_CASE(ty)                                                                             \
   case ty:                                                                                             \
-    fine_apply_kernel<T, ESrc, ty, NZT, CLS><<<grid, threads, fine_smem_bytes<T, ty, NZT>(), st>>>(p); \
+    launch_kernel(pdl, fine_apply_kernel<T, ESrc, ty, NZT, CLS>, grid, dim3(threads),               \
+                  fine_smem_bytes<T, ty, NZT>(), st, p);                                                \
     return TP3D_OK;
     TP3D_FINE_TY_LIST(TP3D_FINE_CASE)
 #undef TP3D_FINE_CASE
@@ -81,9 +83,9 @@ int fine_launch_t(const FineParams<T, ESrc>& p, int TY, dim3 grid, int threads, 
   return TP3D_ERR_ARG;
 }
 template <typename T, class ESrc>
-int fine_launch(const FineParams<T, ESrc>& p, int TY, bool cls, dim3 grid, int threads, cudaStream_t st) {
-  return cls ? fine_launch_t<T, ESrc, true>(p, TY, grid, threads, st)
-             : fine_launch_t<T, ESrc, false>(p, TY, grid, threads, st);
+int fine_launch(const FineParams<T, ESrc>& p, int TY, bool cls, dim3 grid, int threads, cudaStream_t st, bool pdl) {
+  return cls ? fine_launch_t<T, ESrc, true>(p, TY, grid, threads, st, pdl)
+             : fine_launch_t<T, ESrc, false>(p, TY, grid, threads, st, pdl);
 }
 
 template <typename T, class ESrc>
@@ -228,6 +230,11 @@ struct tp3d_solver {
   unsigned int* fin_count = nullptr;  // arrivals of the reduction in flight (last_block_finalize)
   // device-side CG loop (capture_loop)
   bool loop_ok = true, in_loop_capture = false, branch_ok = true;
+  // Programmatic dependent launch (o.pdl; cleared when a graph cannot be
+  // built with it).  Used only while the CG iteration is captured
+  // (pdl_region), and never for the first kernel after a graph entry or a
+  // conditional node (plain_next), so that every such launch follows a kernel.
+  bool pdl = true, pdl_region = false, plain_next = true;
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
   cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
@@ -318,7 +325,7 @@ struct tp3d_solver {
       p.fix = fix[0];
       p.esrc = EFromF64{E64};
       p.io = io;
-      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st, take_pdl(kPdlFine));
     } else if (rho16) {
       FineParams<float, EFromBF16> p;
       p.ke = ke32;
@@ -329,7 +336,7 @@ struct tp3d_solver {
       p.fix = fix[0];
       p.esrc = EFromBF16{rho16, (float)penal};
       p.io = io;
-      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st, take_pdl(kPdlFine));
     } else {
       FineParams<float, EFromF32> p;
       p.ke = ke32;
@@ -340,7 +347,7 @@ struct tp3d_solver {
       p.fix = fix[0];
       p.esrc = EFromF32{E32};
       p.io = io;
-      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st);
+      rc = fine_launch(p, tile.TY, ke_cls, grid, tile.threads, st, take_pdl(kPdlFine));
     }
     if (rc) return rc;
     count_launch();
@@ -357,6 +364,22 @@ struct tp3d_solver {
     if constexpr (sizeof(T) == 8) return wt64;
     else return wt32;
   }
+  // Whether the next loop kernel is launched with the programmatic-serialization
+  // attribute; consumes plain_next.
+  // cls: kPdlCoarse for kernels over a coarse level, kPdlFine for the fine
+  // operator and the fine-level vector kernels (o.pdl is a mask of the two).
+  bool take_pdl(int cls) {
+    const bool on = (o.pdl & cls) && pdl && pdl_region && !plain_next;
+    plain_next = false;
+    return on;
+  }
+  // A loop kernel (it begins with pdl_entry()); errors surface through
+  // cudaGetLastError like a <<<>>> launch.
+  template <typename... P, typename... A>
+  void launch(int cls, void (*k)(P...), dim3 grid, dim3 block, size_t smem, A&&... args) {
+    launch_kernel(take_pdl(cls), k, grid, block, smem, st, static_cast<A&&>(args)...);
+    count_launch();
+  }
   template <typename T, class ESrc>
   int wht_launch_with(int mode, const OpIO<T>& io, const WhtTile& w, ESrc esrc) {
     WhtParams<T, ESrc> p;
@@ -368,7 +391,7 @@ struct tp3d_solver {
     p.fix = fix[0];
     p.esrc = esrc;
     p.io = io;
-    return wht_launch<T, ESrc>(p, mode, w.variant, dim3(w.tiles_y * w.tiles_x, w.zchunks), st);
+    return wht_launch<T, ESrc>(p, mode, w.variant, dim3(w.tiles_y * w.tiles_x, w.zchunks), st, take_pdl(kPdlFine));
   }
   template <typename T>
   int fine_wht_tile(int mode, const OpIO<T>& io, const WhtTile& w) {
@@ -486,8 +509,7 @@ struct tp3d_solver {
     p.S = levels<T>()[L].A;
     p.fix = fix[L];
     p.io = io;
-    stencil_apply_kernel<T, MODE><<<grid_blocks(3 * grids[L].nnode()), 256, 0, st>>>(p);
-    count_launch();
+    launch(kPdlCoarse, stencil_apply_kernel<T, MODE>, dim3(grid_blocks(3 * grids[L].nnode())), dim3(256), 0, p);
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
   }
@@ -627,26 +649,25 @@ struct tp3d_solver {
     const Grid& gl = grids[L];
     const long long ndof = 3 * gl.nnode();
     if (nlev == 1) {  // no hierarchy: Jacobi preconditioner
-      smooth_zero_kernel<T><<<grid_blocks(ndof), 256, 0, st>>>(ndof, b, lv.dinv, T(1), nullptr, lv.x[0], nullptr,
-                                                               done);
-      count_launch();
+      launch(kPdlFine, smooth_zero_kernel<T>, dim3(grid_blocks(ndof)), dim3(256), 0, ndof, b, (const T*)lv.dinv, T(1),
+             (const double*)nullptr, lv.x[0], (T*)nullptr, done);
       return lv.x[0];
     }
     if (L == nlev - 1) {
       const T* inv;
       if constexpr (sizeof(T) == 8) inv = cinv64;
       else inv = cinv32;
-      dense_matvec_kernel<T><<<std::max(1, std::min(cn / 8 + 1, nsm)), 256, 0, st>>>(cn, inv, b, lv.x[0], done);
-      count_launch();
+      launch(kPdlCoarse, dense_matvec_kernel<T>, dim3(std::max(1, std::min(cn / 8 + 1, nsm))), dim3(256), 0, cn, inv,
+             b, lv.x[0], done);
       return lv.x[0];
     }
     if (L == cyc_L0 && cyc_L0 > 0) return coarse_cycle<T>(L, b, rc);
     const bool cheb = o.smoother != 1;
     int cur = 0;
     if (!zero_done) {
-      smooth_zero_kernel<T><<<grid_blocks(ndof), 256, 0, st>>>(ndof, b, lv.dinv, (T)o.omega, cheb ? coef[L] : nullptr,
-                                                               lv.x[cur], cheb ? lv.d : nullptr, done);
-      count_launch();
+      launch(L == 0 ? kPdlFine : kPdlCoarse, smooth_zero_kernel<T>, dim3(grid_blocks(ndof)), dim3(256), 0, ndof, b,
+             (const T*)lv.dinv, (T)o.omega, (const double*)(cheb ? coef[L] : nullptr), lv.x[cur],
+             cheb ? lv.d : (T*)nullptr, done);
     }
     *rc |= smooth_steps<T>(L, 1, pre_sweeps(L) - 1, &cur, b, done);
     {
@@ -669,13 +690,11 @@ struct tp3d_solver {
       fs.x0 = lc.x[0];
       fs.d = cheb ? lc.d : nullptr;
     }
-    restrict_kernel<T><<<plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), 256, 0, st>>>(gl, gn, lv.r, fix[L + 1], lc.b,
-                                                                           done, fs);
-    count_launch();
+    launch(kPdlCoarse, restrict_kernel<T>, plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), dim3(256), 0, gl, gn,
+           (const T*)lv.r, (const uint8_t*)fix[L + 1], lc.b, done, fs);
     T* xc = vcycle<T>(L + 1, lc.b, done, rc, fuse_first);
-    prolong_add_kernel<T><<<plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1), 256, 0, st>>>(gl, gn, xc, fix[L],
-                                                                                             lv.x[cur], done);
-    count_launch();
+    launch(L == 0 ? kPdlFine : kPdlCoarse, prolong_add_kernel<T>, plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1),
+           dim3(256), 0, gl, gn, (const T*)xc, (const uint8_t*)fix[L], lv.x[cur], done);
     const bool dot_here = dot_op >= 0 && o.smoother != 1 && post_sweeps(L) >= 1;
     *rc |= smooth_steps<T>(L, 0, post_sweeps(L), &cur, b, done, dot_here ? dot_op : -1);
     if (dot_here && dot_done) *dot_done = true;
@@ -687,20 +706,28 @@ struct tp3d_solver {
   template <typename T, class Body>
   int capture(KrylovVec<T>& K, Body body) {
     if (K.graph) return TP3D_OK;
-    cudaGraph_t gr;
+    cudaGraph_t gr = nullptr;
     TP3D_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     long long nk = 0;
     t_capture_count = &nk;
+    pdl_region = true;
+    plain_next = true;
     const int rc = body();
+    pdl_region = false;
     t_capture_count = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &gr);
-    if (rc || e != cudaSuccess) {
+    const cudaError_t e2 = (rc || e != cudaSuccess) ? cudaErrorUnknown : cudaGraphInstantiate(&K.graph, gr, 0);
+    if (e == cudaSuccess && gr) cudaGraphDestroy(gr);
+    if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+      cudaGetLastError();
+      K.graph = nullptr;
+      if (pdl) {  // retry in plain stream order
+        pdl = false;
+        return capture<T>(K, body);
+      }
       tp3d_set_last_error("CG graph capture failed");
       return TP3D_ERR_CUDA;
     }
-    const cudaError_t e2 = cudaGraphInstantiate(&K.graph, gr, 0);
-    cudaGraphDestroy(gr);
-    TP3D_CHECK(e2);
     K.graph_kernels = nk;
     return TP3D_OK;
   }
@@ -739,7 +766,10 @@ struct tp3d_solver {
       t_capture_count = &nk;
       in_loop_capture = true;
       branch_count = 0;
+      pdl_region = true;
+      plain_next = true;
       rc = body();
+      pdl_region = false;
       set_loop_cond_kernel<<<1, 1, 0, st>>>(hw, state, loop_passes, (unsigned int)o.max_iterations + 16u);
       ++nk;
       in_loop_capture = false;
@@ -755,6 +785,11 @@ struct tp3d_solver {
     if (!ok) {
       if (K.graph) cudaGraphExecDestroy(K.graph);
       K.graph = nullptr;
+      branch_ok = true;
+      if (pdl) {  // retry in plain stream order
+        pdl = false;
+        return capture_loop<T>(K, body);
+      }
       loop_ok = false;
       return false;
     }
@@ -805,6 +840,7 @@ struct tp3d_solver {
       long long* outer = t_capture_count;
       long long nb = 0;
       t_capture_count = &nb;
+      plain_next = true;
       rc = branch();
       t_capture_count = outer;
       cudaGraph_t out = nullptr;
@@ -815,6 +851,7 @@ struct tp3d_solver {
       branch_count += nb;
     }
     std::swap(st, st_branch);
+    plain_next = true;  // the next kernel follows the IF node
     return rc;
   }
 
@@ -903,15 +940,16 @@ struct tp3d_solver {
     io.fin_count = fin_count;
     int rc = fine<double, kModeCgQ>(io);
     const CoarseFirstStep<double> fs0 = first_step<double>(0);
-    cg_update_kernel<double><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRR, fin_count, fs0);
-    count_launch();
+    launch(kPdlFine, cg_update_kernel<double>, dim3(nb), dim3(256), 0, ndof, K.u, (const double*)K.p, K.r,
+           (const double*)K.q, state, partials, (int)kFinRR, fin_count, fs0);
     bool dot_done = false;
     double* z = vcycle<double>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZ, &dot_done);
     if (!dot_done) {
-      dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZ, fin_count);
-      count_launch();
+      launch(kPdlFine, dot_kernel<double>, dim3(nb), dim3(256), 0, ndof, (const double*)K.r, (const double*)z, partials,
+             (const int*)done, (const int*)nullptr, state, (int)kFinRZ, fin_count);
     }
-    cg_p_kernel<double><<<nb, 256, 0, st>>>(ndof, z, K.p, state, 0); count_launch();
+    launch(kPdlFine, cg_p_kernel<double>, dim3(nb), dim3(256), 0, ndof, (const double*)z, K.p,
+           (const PcgState*)state, 0);
     TP3D_CHECK_LAUNCH();
     return rc;
   }
@@ -1028,13 +1066,12 @@ struct tp3d_solver {
     io.fin_count = fin_count;
     int rc = fine<float, kModeCgQ>(io);
     const CoarseFirstStep<float> fs0 = first_step<float>(0);
-    cg_update_kernel<float><<<nb, 256, 0, st>>>(ndof, K.u, K.p, K.r, K.q, state, partials, kFinRRMixed, fin_count,
-                                                fs0);
-    count_launch();
+    launch(kPdlFine, cg_update_kernel<float>, dim3(nb), dim3(256), 0, ndof, K.u, (const float*)K.p, K.r,
+           (const float*)K.q, state, partials, (int)kFinRRMixed, fin_count, fs0);
     // reliable update (each kernel is also gated on state->update itself)
     rc |= update_branch([&]() {
       int brc = TP3D_OK;
-      flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K.u, state, 0); count_launch();
+      launch(kPdlFine, flush_kernel, dim3(nb), dim3(256), 0, ndof, u64, K.u, (const PcgState*)state, 0);
       OpIO<double> r;
       r.u = u64;
       r.out = r64;
@@ -1042,25 +1079,23 @@ struct tp3d_solver {
       r.done = done;
       r.gate = &state->update;
       brc |= fine<double, kModeResid>(r);
-      dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, done, &state->update, state, kFinRRHi,
-                                             fin_count);
-      count_launch();
-      demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K.r, state, 0); count_launch();
+      launch(kPdlFine, dot_kernel<double>, dim3(nb), dim3(256), 0, ndof, (const double*)r64, (const double*)r64,
+             partials, (const int*)done, (const int*)&state->update, state, (int)kFinRRHi, fin_count);
+      launch(kPdlFine, demote_kernel, dim3(nb), dim3(256), 0, ndof, (const double*)r64, K.r, (const PcgState*)state, 0);
       if (fs0.x0) {  // the first smoothing step again, from the replaced residual
-        smooth_zero_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, fs0.dinv, fs0.omega, fs0.coef, fs0.x0, fs0.d,
-                                                      done);
-        count_launch();
+        launch(kPdlFine, smooth_zero_kernel<float>, dim3(nb), dim3(256), 0, ndof, (const float*)K.r,
+               (const float*)fs0.dinv, fs0.omega, (const double*)fs0.coef, fs0.x0, fs0.d, (const int*)done);
       }
-      clear_update_kernel<<<1, 1, 0, st>>>(state); count_launch();
+      launch(kPdlFine, clear_update_kernel, dim3(1), dim3(1), 0, state);
       return brc;
     });
     bool dot_done = false;
     float* z = vcycle<float>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZMixed, &dot_done);
     if (!dot_done) {
-      dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K.r, z, partials, done, nullptr, state, kFinRZMixed, fin_count);
-      count_launch();
+      launch(kPdlFine, dot_kernel<float>, dim3(nb), dim3(256), 0, ndof, (const float*)K.r, (const float*)z, partials,
+             (const int*)done, (const int*)nullptr, state, (int)kFinRZMixed, fin_count);
     }
-    cg_p_kernel<float><<<nb, 256, 0, st>>>(ndof, z, K.p, state, 0); count_launch();
+    launch(kPdlFine, cg_p_kernel<float>, dim3(nb), dim3(256), 0, ndof, (const float*)z, K.p, (const PcgState*)state, 0);
     TP3D_CHECK_LAUNCH();
     return rc;
   }
@@ -1233,6 +1268,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->coarse_sweeps = 2;
   o->device_loop = 1;
   o->deep_sweeps = 4;
+  o->pdl = 2;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1242,6 +1278,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   tp3d_solver* s = new tp3d_solver();
   if (opts) s->o = *opts;
   else tp3d_solver_default_opts(&s->o);
+  s->pdl = s->o.pdl != 0;
   auto fail = [&](int rc, const char* msg) {
     tp3d_set_last_error(msg);
     delete s;
@@ -1254,6 +1291,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     return fail(TP3D_ERR_ARG, "invalid solver options");
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
+  if (o.pdl < 0 || o.pdl > 3) return fail(TP3D_ERR_ARG, "invalid pdl");
   if (o.smoother != 1 && o.pre_sweeps != o.post_sweeps)
     return fail(TP3D_ERR_ARG, "pre_sweeps and post_sweeps must be equal: the Chebyshev V-cycle preconditions CG and "
                               "must stay symmetric");
@@ -1745,7 +1783,8 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0,
                            s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
                            s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0,
-                           (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0};
+                           (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0,
+                           s->pdl ? (double)s->o.pdl : 0.0};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -170,6 +170,34 @@ def test_fused_coarse_cycle_matches_per_phase_launches(P, dims, smoother, prec):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=tol * np.abs(Us[0]).max())
 
 
+# Programmatic dependent launch only changes when a kernel may be scheduled,
+# never what it computes or in which order the kernels' writes land: every
+# mask gives bit-identical iterations and solutions, with the device loop.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_programmatic_launch_is_bitwise_neutral(P, prec):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 40, 20, 20
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=6, lo=0.0)
+    rho[rho < 0.3] = 0.0
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    its, Us = [], []
+    for mask in (0, 1, 2, 3):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, pdl=mask)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(F)
+        st = s.stats()
+        assert st["pdl"] == mask and st["device_loop"] == 1.0, st
+        its.append(s.last_iterations)
+        Us.append(U.cpu().numpy())
+        s.close()
+    assert len(set(its)) == 1, its
+    for U in Us[1:]:
+        np.testing.assert_array_equal(U, Us[0])
+
+
 # Levels >= 2 from element-wise Galerkin products (default) and from the
 # stencil triple product P^T A P are the same operators up to rounding: same
 # iterations, same solution.  Odd grids exercise the padded coarse elements.
