@@ -178,6 +178,16 @@ typedef struct tp3d_solver_opts {
                            the tail of the one before it), a mask: 1 the coarse levels' kernels,
                            2 the fine operator and fine-level vector kernels, 3 both, 0 plain stream
                            order.  Turned off by itself when a CUDA graph cannot be built with it. */
+  int coarse_bf16;      /* mixed form: levels 1 .. coarse_bf16 (default 99: every level but the
+                           dense coarsest) store their packed stencils in bf16 (symmetrized, FP32
+                           arithmetic), halving the bytes each smoothing step there reads; 0 all
+                           FP32.  The preconditioner only: the CG operator and the
+                           FP64 residuals are unchanged, so the stopping test is too.  Used with
+                           the Chebyshev smoother, whose interval is measured on the operator it
+                           smooths (damped Jacobi's fixed omega has no margin for the rounding). */
+  int split_dofs;       /* coarse levels with at most this many DOFs apply their stencil with four
+                           threads per DOF (more loads in flight on levels too small to fill the
+                           GPU); larger levels one thread per DOF */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -220,8 +230,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * FP64-fallback flag (mixed), fine form of the FP64 operator and of the FP32 operator
  * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent), first level of the fused
  * coarse cycle (0 none), 1 when the CG loop runs on the device (one graph launch per
- * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none).
- * Returns the count written. */
+ * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none),
+ * the number of levels whose stencils are held in bf16.  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

@@ -54,6 +54,8 @@ class SolverOpts(C.Structure):
         ("device_loop", i32),
         ("deep_sweeps", i32),
         ("pdl", i32),
+        ("coarse_bf16", i32),
+        ("split_dofs", i32),
     ]
 
 

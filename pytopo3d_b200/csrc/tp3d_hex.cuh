@@ -221,13 +221,52 @@ __global__ void stencil_pack_kernel(Grid g, const double* __restrict__ A, const 
   }
 }
 
-template <typename T>
+// Packed layout with bf16 coefficients (the mixed form's level-1 option):
+// symmetric by construction, each coupling the mean of its two FP64 copies
+// rounded once, so the operator the FP32 smoother sees stays symmetric.
+template <typename TS>
+__global__ void stencil_pack_sym_kernel(Grid g, const double* __restrict__ A, const uint8_t* __restrict__ fix,
+                                        TS* S) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const long long nn = g.nnode(), ndof = 3 * nn;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ndof; i += (long long)gridDim.x * blockDim.x) {
+    const long long n = i / 3;
+    const int c = (int)(i - 3 * n);
+    const int iy = (int)(n % NY);
+    const long long r = n / NY;
+    const int ix = (int)(r % NX), iz = (int)(r / NX);
+    const bool fi = (fix[n] >> c) & 1;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int x = ix + dx, y = iy + dy, z = iz + dz;
+          const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
+          const long long m = in ? g.nidx(x, y, z) : n;
+          const int fm = in ? fix[m] : 7;
+          const int jr = jrel_of(dx, dy, dz);
+          for (int d = 0; d < 3; ++d) {
+            const double v = (fi || ((fm >> d) & 1))
+                                 ? 0.0
+                                 : 0.5 * (A[(long long)stencil_k(jr, c, d) * nn + n] +
+                                          A[(long long)stencil_k(26 - jr, d, c) * nn + m]);
+            S[(long long)(jr * 3 + d) * ndof + i] = TS(v);
+          }
+        }
+  }
+}
+
+template <typename T, typename TS = T>
 struct StencilParams {
   Grid g;
-  const T* S;  // packed layout
+  const TS* S;  // packed layout
   const uint8_t* fix;
   OpIO<T> io;
 };
+
+template <typename T>
+__device__ __forceinline__ T ld_coef(const T* p) { return __ldg(p); }
+template <typename T>
+__device__ __forceinline__ T ld_coef(const __nv_bfloat16* p) { return (T)__bfloat162float(__ldg(p)); }
 
 // One DOF per thread: 81 coalesced coefficient loads and 81 neighbour loads,
 // all independent (offsets past the grid are clamped to the node itself and
@@ -235,8 +274,8 @@ struct StencilParams {
 // levels hold far fewer than 2^31 DOFs: 32-bit index arithmetic.
 // Row i of the packed stencil times u (K u at DOF i; fixed rows and columns are
 // zero in the packed layout).
-template <typename T>
-__device__ __forceinline__ T stencil_row(const Grid& g, const T* __restrict__ S, const T* __restrict__ u, int i) {
+template <typename T, typename TS = T>
+__device__ __forceinline__ T stencil_row(const Grid& g, const TS* __restrict__ S, const T* __restrict__ u, int i) {
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const int NXY = NX * NY;
   const int ndof = 3 * NXY * NZ;
@@ -257,18 +296,18 @@ __device__ __forceinline__ T stencil_row(const Grid& g, const T* __restrict__ S,
       for (int e = 0; e < 3; ++e) {
         const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
         const int m3 = 3 * (n + oz + ox + oy);
-        const T* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
-        kv = fma(__ldg(s), __ldg(&u[m3]), kv);
-        kv = fma(__ldg(s + ndof), __ldg(&u[m3 + 1]), kv);
-        kv = fma(__ldg(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
+        const TS* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
+        kv = fma(ld_coef<T>(s), __ldg(&u[m3]), kv);
+        kv = fma(ld_coef<T>(s + ndof), __ldg(&u[m3 + 1]), kv);
+        kv = fma(ld_coef<T>(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
       }
     }
   }
   return kv;
 }
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T> p) {
+template <typename T, int MODE, typename TS = T>
+__global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constant__ StencilParams<T, TS> p) {
   pdl_entry();
   if (op_skip(p.io)) return;
   __shared__ double red[32];
@@ -278,9 +317,78 @@ __global__ void __launch_bounds__(256) stencil_apply_kernel(const __grid_constan
   double part = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ndof; i += gridDim.x * blockDim.x) {
     const int n = i / 3, c = i - 3 * n;
-    const T kv = stencil_row<T>(g, p.S, u, i);
+    const T kv = stencil_row<T, TS>(g, p.S, u, i);
     const bool fx = (p.fix[n] >> c) & 1;
     op_epilogue<T, MODE>(p.io, i, fx, kv, fx ? T(0) : u[i], epi_load<T, MODE>(p.io, i), part);
+  }
+  if (mode_reduces<MODE>()) {
+    part = block_sum(part, red);
+    if (threadIdx.x == 0) p.io.partials[blockIdx.x] = part;
+    if (p.io.fin_count) last_block_finalize(p.io.partials, gridDim.x, p.io.fin_count, p.io.fin, p.io.fin_op, red);
+  }
+}
+
+// The same operator with four lanes per DOF, for the small coarse levels,
+// where a launch holds too few threads to keep the memory system busy and each
+// thread's 162 loads are the critical path: lane q of a group of four
+// multiplies neighbours 7q .. 7q+6 of the 27 (in stencil_row's z, x, y order),
+// the group adds its partial sums with two xor shuffles and its first lane
+// runs the epilogue.  The loop bound is uniform over each block, so every lane
+// reaches the shuffles.
+template <typename T, typename TS>
+__device__ __forceinline__ T stencil_row_part(const Grid& g, const TS* __restrict__ S, const T* __restrict__ u, int i,
+                                              int q) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const int NXY = NX * NY;
+  const int ndof = 3 * NXY * NZ;
+  const int n = i / 3;
+  const int iy = n % NY, r = n / NY;
+  const int ix = r % NX, iz = r / NX;
+  const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
+  const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
+  const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
+  T kv = T(0);
+#pragma unroll
+  for (int jj = 0; jj < 7; ++jj) {
+    const int j = 7 * q + jj;
+    if (j < 27) {
+      const int a = j / 9, b = (j / 3) % 3, e = j % 3;
+      const int oz = a == 0 ? oz0 : (a == 1 ? 0 : oz2);
+      const int ox = b == 0 ? ox0 : (b == 1 ? 0 : ox2);
+      const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
+      const int m3 = 3 * (n + oz + ox + oy);
+      const TS* s = S + (size_t)(j * 3) * ndof + i;
+      kv = fma(ld_coef<T>(s), __ldg(&u[m3]), kv);
+      kv = fma(ld_coef<T>(s + ndof), __ldg(&u[m3 + 1]), kv);
+      kv = fma(ld_coef<T>(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
+    }
+  }
+  return kv;
+}
+
+template <typename T, int MODE, typename TS = T>
+__global__ void __launch_bounds__(256) stencil_apply4_kernel(const __grid_constant__ StencilParams<T, TS> p) {
+  pdl_entry();
+  if (op_skip(p.io)) return;
+  __shared__ double red[32];
+  const Grid g = p.g;
+  const int ndof = 3 * (g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+  const T* __restrict__ u = p.io.u;
+  const int q = threadIdx.x & 3;
+  double part = 0.0;
+  for (int base = blockIdx.x * blockDim.x; base < 4 * ndof; base += gridDim.x * blockDim.x) {
+    const int i = (base + threadIdx.x) >> 2;
+    const bool live = i < ndof;
+    EpiIn<T> in;
+    if (live && q == 0) in = epi_load<T, MODE>(p.io, i);
+    T kv = live ? stencil_row_part<T, TS>(g, p.S, u, i, q) : T(0);
+    kv += __shfl_xor_sync(0xffffffffu, kv, 1);
+    kv += __shfl_xor_sync(0xffffffffu, kv, 2);
+    if (live && q == 0) {
+      const int n = i / 3, c = i - 3 * n;
+      const bool fx = (p.fix[n] >> c) & 1;
+      op_epilogue<T, MODE>(p.io, i, fx, kv, fx ? T(0) : u[i], in, part);
+    }
   }
   if (mode_reduces<MODE>()) {
     part = block_sum(part, red);

@@ -235,6 +235,7 @@ struct tp3d_solver {
   // (pdl_region), and never for the first kernel after a graph entry or a
   // conditional node (plain_next), so that every such launch follows a kernel.
   bool pdl = true, pdl_region = false, plain_next = true;
+  std::vector<__nv_bfloat16*> S16;  // packed stencils in bf16 of levels 1 .. o.coarse_bf16 (mixed form), or null
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
   cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
@@ -267,8 +268,8 @@ struct tp3d_solver {
   template <typename T>
   T* alloc(size_t n) {
     void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
-    allocs.push_back(p);
+    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) p = nullptr;
+    allocs.push_back(p);  // a failure is recorded too: create() checks the list
     return (T*)p;
   }
   ~tp3d_solver() {
@@ -504,12 +505,32 @@ struct tp3d_solver {
   template <typename T, int MODE>
   int apply_level(int L, const OpIO<T>& io) {
     if (L == 0) return fine<T, MODE>(io);
+    const long long ndof = 3 * grids[L].nnode();
+    const bool split = ndof <= o.split_dofs;  // four lanes per DOF on the small levels
+    if constexpr (sizeof(T) == 4) {
+      if (L < (int)S16.size() && S16[L]) {
+        StencilParams<float, __nv_bfloat16> p;
+        p.g = grids[L];
+        p.S = S16[L];
+        p.fix = fix[L];
+        p.io = io;
+        if (split)
+          launch(kPdlCoarse, stencil_apply4_kernel<float, MODE, __nv_bfloat16>, dim3(grid_blocks(4 * ndof)),
+                 dim3(256), 0, p);
+        else
+          launch(kPdlCoarse, stencil_apply_kernel<float, MODE, __nv_bfloat16>, dim3(grid_blocks(ndof)), dim3(256), 0,
+                 p);
+        TP3D_CHECK_LAUNCH();
+        return TP3D_OK;
+      }
+    }
     StencilParams<T> p;
     p.g = grids[L];
     p.S = levels<T>()[L].A;
     p.fix = fix[L];
     p.io = io;
-    launch(kPdlCoarse, stencil_apply_kernel<T, MODE>, dim3(grid_blocks(3 * grids[L].nnode())), dim3(256), 0, p);
+    if (split) launch(kPdlCoarse, stencil_apply4_kernel<T, MODE>, dim3(grid_blocks(4 * ndof)), dim3(256), 0, p);
+    else launch(kPdlCoarse, stencil_apply_kernel<T, MODE>, dim3(grid_blocks(ndof)), dim3(256), 0, p);
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
   }
@@ -1269,6 +1290,8 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->device_loop = 1;
   o->deep_sweeps = 4;
   o->pdl = 2;
+  o->coarse_bf16 = 99;
+  o->split_dofs = 16384;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1292,6 +1315,8 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
   if (o.pdl < 0 || o.pdl > 3) return fail(TP3D_ERR_ARG, "invalid pdl");
+  if (o.split_dofs < 0) return fail(TP3D_ERR_ARG, "invalid split_dofs");
+  if (o.coarse_bf16 < 0) return fail(TP3D_ERR_ARG, "invalid coarse_bf16");
   if (o.smoother != 1 && o.pre_sweeps != o.post_sweeps)
     return fail(TP3D_ERR_ARG, "pre_sweeps and post_sweeps must be equal: the Chebyshev V-cycle preconditions CG and "
                               "must stay symmetric");
@@ -1407,6 +1432,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     for (int L = 2; L < s->nlev; ++L) s->Kel[L] = s->alloc<double>((size_t)576 * s->grids[L].nele());
   }
   s->A64.assign(s->nlev, nullptr);
+  s->S16.assign(s->nlev, nullptr);
   s->L64.resize(s->nlev);
   if (mixed) s->L32.resize(s->nlev);
   for (int L = 0; L < s->nlev; ++L) {
@@ -1424,7 +1450,14 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       b.x[0] = s->alloc<float>(ndof); b.x[1] = s->alloc<float>(ndof);
       b.b = s->alloc<float>(ndof); b.r = s->alloc<float>(ndof); b.d = s->alloc<float>(ndof);
       b.dinv = s->alloc<float>(ndof);
-      if (L > 0) b.A = s->alloc<float>(243 * nn);
+      // bf16 stencils with the Chebyshev smoother only: its interval comes from
+      // the operator's own power iteration, whereas damped Jacobi's fixed omega
+      // leaves omega lambda_max(Dinv A) near 2 with no margin for the rounding.
+      // Not on the dense coarsest level, nor inside a fused coarse cycle.
+      const bool bf16 = L >= 1 && L <= s->o.coarse_bf16 && s->o.smoother != 1 && L < s->nlev - 1 &&
+                        !(s->cyc_L0 > 0 && L >= s->cyc_L0);
+      if (bf16) s->S16[L] = s->alloc<__nv_bfloat16>(243 * nn);
+      else if (L > 0) b.A = s->alloc<float>(243 * nn);
     }
   }
   s->cn = (int)(3 * s->grids.back().nnode());
@@ -1570,7 +1603,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     const unsigned nb = (unsigned)((gc.nnode() + 31) / 32);
     if (L == 2 && elem_chain) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
     // the builders also write the packed (apply) layout of the solve's precision
-    float* P32 = mixed ? s->L32[L].A : nullptr;
+    float* P32 = mixed && !s->S16[L] ? s->L32[L].A : nullptr;
     double* P64 = mixed ? nullptr : s->L64[L].A;
     bool packed = true;
     if (L == 1) {
@@ -1590,7 +1623,13 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     if (mixed) {
       convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
       count_launch();
-      if (!packed) s->pack_level<float>(L, s->L32[L].A);
+      if (s->S16[L]) {
+        stencil_pack_sym_kernel<__nv_bfloat16><<<s->grid_blocks(3 * nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L],
+                                                                                        s->S16[L]);
+        count_launch();
+      } else if (!packed) {
+        s->pack_level<float>(L, s->L32[L].A);
+      }
       if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // the mixed form's FP64 fallback
     } else if (!packed) {
       s->pack_level<double>(L, s->L64[L].A);
@@ -1784,7 +1823,8 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
                            s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0,
                            (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0,
-                           s->pdl ? (double)s->o.pdl : 0.0};
+                           s->pdl ? (double)s->o.pdl : 0.0,
+                           (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; })};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

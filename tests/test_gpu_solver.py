@@ -104,7 +104,10 @@ def test_fp64_solve_matches_reference_direct_solve(P, golden, tag):
 # given; either way its compliance must stay within 1e-6 of the FP64 form's.
 @pytest.mark.parametrize("dims,opts", [((16, 8, 8), {}), ((24, 12, 12), {}), ((20, 7, 9), {}),
                                        ((24, 12, 12), {"inner_density": 1}), ((16, 8, 8), {"rtol": 1e-10}),
-                                       ((24, 12, 12), {"inner_density": 1, "rtol": 1e-10})])
+                                       ((24, 12, 12), {"inner_density": 1, "rtol": 1e-10}),
+                                       ((24, 12, 12), {"coarse_bf16": 0}), ((40, 20, 20), {"coarse_bf16": 1}),
+                                       ((16, 8, 8), {"coarse_bf16": 1, "rtol": 1e-10}),
+                                       ((40, 20, 20), {"coarse_bf16": 4})])
 def test_mixed_precision_matches_fp64(P, dims, opts):
     from pytopo3d_b200._tensors import to_flat
     from pytopo3d_b200.solver import HexSolver
@@ -126,6 +129,10 @@ def test_mixed_precision_matches_fp64(P, dims, opts):
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
         assert s.stats()["device_loop"] == 1.0  # one graph launch per solve, no host polling
+        st = s.stats()
+        # bf16 stencils on levels 1 .. coarse_bf16, never on the dense coarsest level
+        n16 = max(0, min(opts.get("coarse_bf16", 99), int(st["levels"]) - 2)) if prec == "mixed" else 0
+        assert st["coarse_bf16"] == n16, st
         # 1e-9 void pockets put an attainable floor on the true residual; the
         # solver accepts it only once restarts / reliable updates stop gaining
         assert s.last_relres <= rtol or (s.stats()["residual_floor"] and s.last_relres <= max(rtol, 1e-7))
@@ -155,7 +162,9 @@ def test_fused_coarse_cycle_matches_per_phase_launches(P, dims, smoother, prec):
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
     its, Us = [], []
     for fused in (0, 65536):
-        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, fused_cycle_dofs=fused, smoother=smoother)
+        # one thread per DOF on every level: the fused cycle's order of additions
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, fused_cycle_dofs=fused, smoother=smoother,
+                      split_dofs=0)
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
         st = s.stats()
@@ -170,9 +179,38 @@ def test_fused_coarse_cycle_matches_per_phase_launches(P, dims, smoother, prec):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=tol * np.abs(Us[0]).max())
 
 
+# The small levels' stencil with four lanes per DOF is the same operator as
+# one thread per DOF, summed in another order: same iterations (within one or
+# 2%), same solution to rounding.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims", [(48, 24, 24), (20, 7, 9), (33, 17, 9)])
+def test_split_stencil_matches_one_thread_per_dof(P, dims, prec):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=7, lo=0.0)
+    rho[rho < 0.25] = 0.0
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    its, Us = [], []
+    for split in (0, 1 << 30):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, split_dofs=split, fine_operator=3)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(F)
+        its.append(s.last_iterations)
+        Us.append(U.cpu().numpy())
+        s.close()
+    assert abs(its[0] - its[1]) <= max(1, 0.02 * its[0]), its
+    tol = 1e-9 if prec == "fp64" else 1e-5
+    np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=tol * np.abs(Us[0]).max())
+
+
 # Programmatic dependent launch only changes when a kernel may be scheduled,
 # never what it computes or in which order the kernels' writes land: every
 # mask gives bit-identical iterations and solutions, with the device loop.
+# (The fine operator's launch shape is fixed: the timed choice may pick
+# another shape per solver, which rounds differently.)
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_programmatic_launch_is_bitwise_neutral(P, prec):
     from pytopo3d_b200._tensors import to_flat
@@ -185,7 +223,7 @@ def test_programmatic_launch_is_bitwise_neutral(P, prec):
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
     its, Us = [], []
     for mask in (0, 1, 2, 3):
-        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, pdl=mask)
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, pdl=mask, fine_operator=3)
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
         st = s.stats()
