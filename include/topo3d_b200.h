@@ -231,7 +231,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * (0 dense, 1 + shape for the Walsh-Hadamard form, -1 absent), first level of the fused
  * coarse cycle (0 none), 1 when the CG loop runs on the device (one graph launch per
  * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none),
- * the number of levels whose stencils are held in bf16.  Returns the count written. */
+ * the number of levels whose stencils are held in bf16, the coarsest inverse's status (0 first
+ * attempt, 1-3 attempts with a raised diagonal, 4 diagonal fallback).  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

@@ -405,12 +405,35 @@ __global__ void dense_from_stencil_kernel(Grid g, const double* __restrict__ A, 
   }
 }
 
-// In-place Gauss-Jordan inverse of the SPD matrix D (n x n, row-major) into
-// Inv, one block, no pivoting (SPD pivots stay positive in exact arithmetic).
-// When `in_smem`, the matrix lives in dynamic shared memory (n <= 160).
-// Each pivot step copies row k and column k aside, then updates every entry
-// in one pass over the matrix, a warp per row (two barriers per step).
-// *status = 0 ok, k+1 if pivot k was not positive.
+// Dense inverse of the coarsest operator, entirely on the device (no host
+// round trip per set-up).  Gauss-Jordan without pivoting (SPD pivots stay
+// positive in exact arithmetic); if a pivot is not positive, the elimination
+// restarts from D with the diagonal raised by 1e-12, 1e-9, then 1e-6 times its
+// mean magnitude; if all of those fail too, Inv is the inverse diagonal of D.
+// *status = the number of shifted attempts used (0..3), or kGjFallback.
+constexpr int kGjAttempts = 4;
+constexpr int kGjFallback = 4;
+
+__device__ __forceinline__ double gj_shift(const double* __restrict__ D, int n, int attempt) {
+  if (attempt == 0) return 0.0;
+  double m = 0.0;
+  for (int i = 0; i < n; ++i) m += fabs(D[(size_t)i * n + i]);
+  m = fmax(m / n, 1e-300);
+  return (attempt == 1 ? 1e-12 : (attempt == 2 ? 1e-9 : 1e-6)) * m;
+}
+
+__device__ __forceinline__ void gj_diag_fallback(const double* __restrict__ D, int n, double* Inv) {
+  for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
+    const int i = (int)(t / n), j = (int)(t % n);
+    const double d = D[(size_t)i * n + i];
+    Inv[t] = (i == j && d > 0.0) ? 1.0 / d : 0.0;
+  }
+}
+
+// One block.  When `in_smem`, the working matrix lives in dynamic shared
+// memory (n <= 160), else in Inv.  Each pivot step copies row k and column k
+// aside, then updates every entry in one pass over the matrix, a warp per row
+// (two barriers per step).
 __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const double* __restrict__ D, double* Inv,
                                                                 int in_smem, int* status) {
   extern __shared__ double sA[];  // [n * n if in_smem] [row k: n] [column k: n]
@@ -420,41 +443,51 @@ __global__ void __launch_bounds__(1024) dense_gj_inverse_kernel(int n, const dou
   double* colk = rowk + n;
   __shared__ int bad;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (long long t = threadIdx.x; t < nn; t += blockDim.x) A[t] = D[t];
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int k = 0; k < n; ++k) {
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      rowk[t] = A[(size_t)k * n + t];
-      colk[t] = A[(size_t)t * n + k];
-    }
+  int attempt = 0;
+  for (; attempt < kGjAttempts; ++attempt) {
+    const double shift = gj_shift(D, n, attempt);
+    for (long long t = threadIdx.x; t < nn; t += blockDim.x) A[t] = D[t] + ((t % (n + 1)) == 0 ? shift : 0.0);
+    if (threadIdx.x == 0) bad = 0;
     __syncthreads();
-    const double p = rowk[k];
-    if (threadIdx.x == 0 && !(p > 0.0) && !bad) bad = k + 1;
-    const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
-    // a warp per row, lanes along the row
-    for (int i = warp; i < n; i += nwarps) {
-      double* Ai = A + (size_t)i * n;
-      const double f = colk[i] * pk;
-      if (i == k) {
-        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? pk : rowk[j] * pk;
-      } else {
-        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? -f : Ai[j] - f * rowk[j];
+    for (int k = 0; k < n; ++k) {
+      for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        rowk[t] = A[(size_t)k * n + t];
+        colk[t] = A[(size_t)t * n + k];
       }
+      __syncthreads();
+      const double p = rowk[k];
+      if (threadIdx.x == 0 && !(p > 0.0) && !bad) bad = k + 1;
+      const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
+      // a warp per row, lanes along the row
+      for (int i = warp; i < n; i += nwarps) {
+        double* Ai = A + (size_t)i * n;
+        const double f = colk[i] * pk;
+        if (i == k) {
+          for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? pk : rowk[j] * pk;
+        } else {
+          for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? -f : Ai[j] - f * rowk[j];
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    const int failed = bad;
+    __syncthreads();  // every thread has read `bad` before thread 0 resets it
+    if (!failed) break;
   }
-  if (in_smem)
+  if (attempt == kGjAttempts) {
+    gj_diag_fallback(D, n, Inv);
+  } else if (in_smem) {
     for (long long t = threadIdx.x; t < nn; t += blockDim.x) Inv[t] = A[t];
-  if (threadIdx.x == 0) *status = bad;
+  }
+  if (threadIdx.x == 0) *status = attempt == kGjAttempts ? kGjFallback : attempt;
 }
 
 // Gauss-Jordan inverse of a small SPD matrix (n <= 160) held in registers: one
 // block of 16 x 32 threads, thread (w, l) owns the 10 x 5 entries (w + 16 r,
 // l + 32 c).  Per pivot step the owners of row k and column k publish them in
 // shared memory (double-buffered, one barrier per step) and every thread
-// updates its entries in registers.  Same arithmetic as
-// dense_gj_inverse_kernel.  *status = 0 ok, k+1 if pivot k was not positive.
+// updates its entries in registers.  Same arithmetic, attempts and status as
+// dense_gj_inverse_kernel.
 constexpr int kGjRegMaxN = 160;
 
 __global__ void __launch_bounds__(512, 1) dense_gj_inverse_reg_kernel(int n, const double* __restrict__ D, double* Inv,
@@ -463,67 +496,77 @@ __global__ void __launch_bounds__(512, 1) dense_gj_inverse_reg_kernel(int n, con
   __shared__ double rowk[2][kGjRegMaxN], colk[2][kGjRegMaxN];
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   double a[R][C];
+  int attempt = 0;
+  for (; attempt < kGjAttempts; ++attempt) {
+    const double shift = gj_shift(D, n, attempt);
 #pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const int i = w + 16 * r, j = l + 32 * c;
-      a[r][c] = (i < n && j < n) ? D[(size_t)i * n + j] : 0.0;
-    }
-  int bad = 0;
-  for (int k = 0; k < n; ++k) {
-    const int buf = k & 1;
-    // owners of row k (warp k % 16, r = k / 16) and of column k (lane k % 32,
-    // c = k / 32) publish them; selects keep every index compile-time
-    if (w == (k & 15)) {
-      const int kr = k >> 4;
+    for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int c = 0; c < C; ++c) {
-        double v = 0.0;
-#pragma unroll
-        for (int r = 0; r < R; ++r) v = (r == kr) ? a[r][c] : v;
-        rowk[buf][l + 32 * c] = v;
+        const int i = w + 16 * r, j = l + 32 * c;
+        a[r][c] = (i < n && j < n) ? D[(size_t)i * n + j] + (i == j ? shift : 0.0) : 0.0;
       }
-    }
-    if (l == (k & 31)) {
-      const int kc = k >> 5;
+    int bad = 0;  // the same in every thread: each reads the pivot from shared memory
+    for (int k = 0; k < n; ++k) {
+      const int buf = k & 1;
+      // owners of row k (warp k % 16, r = k / 16) and of column k (lane k % 32,
+      // c = k / 32) publish them; selects keep every index compile-time
+      if (w == (k & 15)) {
+        const int kr = k >> 4;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          double v = 0.0;
+#pragma unroll
+          for (int r = 0; r < R; ++r) v = (r == kr) ? a[r][c] : v;
+          rowk[buf][l + 32 * c] = v;
+        }
+      }
+      if (l == (k & 31)) {
+        const int kc = k >> 5;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          double v = 0.0;
+#pragma unroll
+          for (int c = 0; c < C; ++c) v = (c == kc) ? a[r][c] : v;
+          colk[buf][w + 16 * r] = v;
+        }
+      }
+      __syncthreads();
+      const double p = rowk[buf][k];
+      if (!(p > 0.0) && !bad) bad = k + 1;
+      const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
+      double g[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) g[c] = rowk[buf][l + 32 * c];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        double v = 0.0;
+        const bool rk = (w + 16 * r) == k;
+        const double f = colk[buf][w + 16 * r] * pk;
 #pragma unroll
-        for (int c = 0; c < C; ++c) v = (c == kc) ? a[r][c] : v;
-        colk[buf][w + 16 * r] = v;
+        for (int c = 0; c < C; ++c) {
+          const bool ck = (l + 32 * c) == k;
+          double v = a[r][c] - f * g[c];
+          if (ck) v = -f;
+          if (rk) v = ck ? pk : g[c] * pk;
+          a[r][c] = v;
+        }
       }
     }
-    __syncthreads();
-    const double p = rowk[buf][k];
-    if (!(p > 0.0) && !bad) bad = k + 1;
-    const double pk = 1.0 / (p > 0.0 ? p : 1e-300);
-    double g[C];
+    __syncthreads();  // the last step's buffers are read before the next attempt writes them
+    if (!bad) break;
+  }
+  if (attempt == kGjAttempts) {
+    gj_diag_fallback(D, n, Inv);
+  } else {
 #pragma unroll
-    for (int c = 0; c < C; ++c) g[c] = rowk[buf][l + 32 * c];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const bool rk = (w + 16 * r) == k;
-      const double f = colk[buf][w + 16 * r] * pk;
+    for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int c = 0; c < C; ++c) {
-        const bool ck = (l + 32 * c) == k;
-        double v = a[r][c] - f * g[c];
-        if (ck) v = -f;
-        if (rk) v = ck ? pk : g[c] * pk;
-        a[r][c] = v;
+        const int i = w + 16 * r, j = l + 32 * c;
+        if (i < n && j < n) Inv[(size_t)i * n + j] = a[r][c];
       }
-    }
   }
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const int i = w + 16 * r, j = l + 32 * c;
-      if (i < n && j < n) Inv[(size_t)i * n + j] = a[r][c];
-    }
-  if (threadIdx.x == 0) *status = bad;
+  if (threadIdx.x == 0) *status = attempt == kGjAttempts ? kGjFallback : attempt;
 }
 
 template <typename T>

@@ -171,20 +171,6 @@ __global__ void convert_kernel(long long n, const Tsrc* __restrict__ a, Tdst* b)
     b[i] = (Tdst)a[i];
 }
 
-__global__ void dense_shift_kernel(int n, double* D, double shift) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) D[(size_t)i * n + i] += shift;
-}
-
-// Fallback coarsest "inverse": the inverse diagonal of the masked dense operator.
-__global__ void dense_diag_inverse_kernel(int n, const double* __restrict__ Dorig, double* Inv) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / n), j = (int)(t % n);
-    const double d = Dorig[(size_t)i * n + i];
-    Inv[t] = (i == j && d > 0.0) ? 1.0 / d : 0.0;
-  }
-}
-
 // Deterministic pseudo-random start vector on free DOFs (power iteration).
 template <typename T>
 __global__ void random_vector_kernel(long long nn, const uint8_t* __restrict__ fix, T* v) {

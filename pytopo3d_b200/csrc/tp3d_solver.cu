@@ -209,7 +209,6 @@ struct tp3d_solver {
   double *cdense = nullptr, *cinv64 = nullptr;
   float* cinv32 = nullptr;
   int* cstatus = nullptr;
-  bool coarse_fallback = false;
 
   double* E64 = nullptr;
   float* E32 = nullptr;
@@ -239,8 +238,7 @@ struct tp3d_solver {
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
   cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
-  cudaEvent_t ev_side_in = nullptr, ev_side_out = nullptr;
-  int* cstatus_host = nullptr;        // pinned copy of the inverse's status
+  cudaEvent_t ev_side_in = nullptr, ev_side_out = nullptr, ev_side_elem = nullptr;
   unsigned int* loop_passes = nullptr;
   unsigned int* loop_pass_host = nullptr;
   PcgState* state = nullptr;
@@ -283,7 +281,7 @@ struct tp3d_solver {
     if (st_side) cudaStreamDestroy(st_side);
     if (ev_side_in) cudaEventDestroy(ev_side_in);
     if (ev_side_out) cudaEventDestroy(ev_side_out);
-    if (cstatus_host) cudaFreeHost(cstatus_host);
+    if (ev_side_elem) cudaEventDestroy(ev_side_elem);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     if (st) cudaStreamDestroy(st);
@@ -1390,7 +1388,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_side_in, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_side_out, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost(&s->cstatus_host, sizeof(int)) != cudaSuccess)
+      cudaEventCreateWithFlags(&s->ev_side_elem, cudaEventDisableTiming) != cudaSuccess)
     return fail(TP3D_ERR_CUDA, "solver setup failed");
   s->state = s->alloc<PcgState>(1);
   unsigned int* cnt = s->alloc<unsigned int>(4);
@@ -1583,72 +1581,16 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       if (int rc = s->choose_fine_form<float>()) return rc;
     s->fine_chosen = true;
   }
-  // Element matrices of levels >= 2 depend only on the fine moduli: they are
-  // built on the side stream while level 1 is built here.
-  const bool elem_chain = s->o.galerkin == 0 && s->nlev > 2;
-  if (elem_chain) {
-    TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
-    TP3D_CHECK(cudaStreamWaitEvent(s->st_side, s->ev_side_in, 0));
-    for (int L = 2; L < s->nlev; ++L) {
-      const unsigned ne = (unsigned)s->grids[L].nele();
-      if (L == 2) elem2_from_fine_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[0], s->grids[2], s->E64, s->KE2, s->Kel[2]);
-      else elem_coarsen_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[L - 1], s->grids[L], s->Kel[L - 1], s->Kel[L]);
-      count_launch();
-    }
-    TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
-  }
-  for (int L = 1; L < s->nlev; ++L) {
-    const Grid& gf = s->grids[L - 1];
-    const Grid& gc = s->grids[L];
-    const unsigned nb = (unsigned)((gc.nnode() + 31) / 32);
-    if (L == 2 && elem_chain) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
-    // the builders also write the packed (apply) layout of the solve's precision
-    float* P32 = mixed && !s->S16[L] ? s->L32[L].A : nullptr;
-    double* P64 = mixed ? nullptr : s->L64[L].A;
-    bool packed = true;
-    if (L == 1) {
-      if (mixed) build_level1_kernel<float><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P32);
-      else build_level1_kernel<double><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P64);
-    } else if (s->o.galerkin == 0) {
-      if (mixed) stencil_from_elems_kernel<float><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P32);
-      else stencil_from_elems_kernel<double><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P64);
-    } else {
-      rap_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->A64[L - 1], s->A64[L]);
-      packed = false;
-    }
-    count_launch();
-    const long long nn = gc.nnode();
-    stencil_diag_inv_kernel<double><<<s->grid_blocks(nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->L64[L].dinv);
-    count_launch();
-    if (mixed) {
-      convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
-      count_launch();
-      if (s->S16[L]) {
-        stencil_pack_sym_kernel<__nv_bfloat16><<<s->grid_blocks(3 * nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L],
-                                                                                        s->S16[L]);
-        count_launch();
-      } else if (!packed) {
-        s->pack_level<float>(L, s->L32[L].A);
-      }
-      if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // the mixed form's FP64 fallback
-    } else if (!packed) {
-      s->pack_level<double>(L, s->L64[L].A);
-    }
-    TP3D_CHECK_LAUNCH();
-  }
-  // The coarsest inverse (one block) runs on a side stream while the power
-  // iterations below use the rest of the GPU; its status is read after both.
-  auto coarsest_gj = [&](cudaStream_t cs, double shift) -> int {
+  // The coarsest inverse (one block) runs on a side stream while the level
+  // builds and the power iterations use the rest of the GPU; its status is read
+  // after both.
+  auto coarsest_gj = [&](cudaStream_t cs) -> int {
     const int L = s->nlev - 1;
     const int n = s->cn;
     TP3D_CHECK(cudaMemsetAsync(s->cdense, 0, (size_t)n * n * sizeof(double), cs));
     dense_from_stencil_kernel<<<s->grid_blocks(s->grids[L].nnode()), 256, 0, cs>>>(s->grids[L], s->A64[L], s->fix[L],
                                                                                     s->cdense);
     count_launch();
-    if (shift > 0.0) {
-      dense_shift_kernel<<<s->grid_blocks(n), 256, 0, cs>>>(n, s->cdense, shift);
-      count_launch();
-    }
     if (n <= kGjRegMaxN) {
       dense_gj_inverse_reg_kernel<<<1, 512, 0, cs>>>(n, s->cdense, s->cinv64, s->cstatus);
       count_launch();
@@ -1665,79 +1607,88 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
                                                                                       s->cinv32);
       count_launch();
     }
-    TP3D_CHECK(cudaMemcpyAsync(s->cstatus_host, s->cstatus, sizeof(int), cudaMemcpyDeviceToHost, cs));
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
   };
-  if (s->nlev > 1) {
+  // Element matrices of levels >= 2 depend only on the fine moduli: they are
+  // built on the side stream while level 1 is built here, and the coarsest
+  // level's stencil and dense inverse follow them there.
+  const bool elem_chain = s->o.galerkin == 0 && s->nlev > 2;
+  const int Lc = s->nlev - 1;
+  if (elem_chain) {
     TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
     TP3D_CHECK(cudaStreamWaitEvent(s->st_side, s->ev_side_in, 0));
-    if (int rc = coarsest_gj(s->st_side, 0.0)) return rc;
+    for (int L = 2; L < s->nlev; ++L) {
+      const unsigned ne = (unsigned)s->grids[L].nele();
+      if (L == 2) elem2_from_fine_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[0], s->grids[2], s->E64, s->KE2, s->Kel[2]);
+      else elem_coarsen_kernel<<<ne, 576, 0, s->st_side>>>(s->grids[L - 1], s->grids[L], s->Kel[L - 1], s->Kel[L]);
+      count_launch();
+    }
+    TP3D_CHECK(cudaEventRecord(s->ev_side_elem, s->st_side));
+    const Grid& gc = s->grids[Lc];
+    const long long nn = gc.nnode();
+    stencil_from_elems_kernel<float><<<(unsigned)((nn + 31) / 32), kBuildThreads, 0, s->st_side>>>(
+        gc, s->Kel[Lc], s->A64[Lc], s->fix[Lc], nullptr);
+    stencil_diag_inv_kernel<double><<<s->grid_blocks(nn), 256, 0, s->st_side>>>(gc, s->A64[Lc], s->fix[Lc],
+                                                                                 s->L64[Lc].dinv);
+    count_launch();
+    count_launch();
+    if (int rc = coarsest_gj(s->st_side)) return rc;
+    TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
+  }
+  for (int L = 1; L < (elem_chain ? Lc : s->nlev); ++L) {
+    const Grid& gf = s->grids[L - 1];
+    const Grid& gc = s->grids[L];
+    const unsigned nb = (unsigned)((gc.nnode() + 31) / 32);
+    if (L == 2 && elem_chain) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_elem, 0));
+    // the builders also write the packed (apply) layout of the solve's
+    // precision (bf16 where the level holds its stencil in bf16)
+    float* P32 = mixed && !s->S16[L] ? s->L32[L].A : nullptr;
+    double* P64 = mixed ? nullptr : s->L64[L].A;
+    __nv_bfloat16* P16 = s->S16[L];
+    bool packed = true;
+    if (L == 1) {
+      if (P16) build_level1_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P16);
+      else if (mixed) build_level1_kernel<float><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P32);
+      else build_level1_kernel<double><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P64);
+    } else if (s->o.galerkin == 0) {
+      if (P16) stencil_from_elems_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P16);
+      else if (mixed) stencil_from_elems_kernel<float><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P32);
+      else stencil_from_elems_kernel<double><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P64);
+    } else {
+      rap_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->A64[L - 1], s->A64[L]);
+      packed = false;
+    }
+    count_launch();
+    const long long nn = gc.nnode();
+    stencil_diag_inv_kernel<double><<<s->grid_blocks(nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->L64[L].dinv);
+    count_launch();
+    if (mixed) {
+      convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
+      count_launch();
+      if (!packed && P16) {
+        stencil_pack_sym_kernel<__nv_bfloat16><<<s->grid_blocks(3 * nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L], P16);
+        count_launch();
+      } else if (!packed) {
+        s->pack_level<float>(L, s->L32[L].A);
+      }
+      if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // the mixed form's FP64 fallback
+    } else if (!packed) {
+      s->pack_level<double>(L, s->L64[L].A);
+    }
+    TP3D_CHECK_LAUNCH();
+  }
+  if (s->nlev > 1 && !elem_chain) {
+    TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
+    TP3D_CHECK(cudaStreamWaitEvent(s->st_side, s->ev_side_in, 0));
+    if (int rc = coarsest_gj(s->st_side)) return rc;
     TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
   }
   if (s->o.smoother != 1)
     if (int rc = mixed ? estimate_spectra<float>(s) : estimate_spectra<double>(s)) return rc;
-  if (s->nlev > 1) {
-    TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
-    TP3D_CHECK(cudaEventSynchronize(s->ev_side_out));
-  }
-  if (s->nlev > 1 && *s->cstatus_host != 0) {
-    const int L = s->nlev - 1;
-    const int n = s->cn;
-    double shift = 0.0;
-    s->coarse_fallback = false;
-    int status = 1;
-    // the unshifted attempt failed: retry with shifts on the solver's stream
-    for (int attempt = 0; attempt < 3 && status != 0; ++attempt) {
-      {
-        std::vector<double> h((size_t)243 * s->grids[L].nnode());
-        cudaMemcpy(h.data(), s->A64[L], h.size() * sizeof(double), cudaMemcpyDeviceToHost);
-        const long long nnL = s->grids[L].nnode();
-        double dsum = 0.0;
-        for (long long i = 0; i < nnL; ++i)
-          for (int c = 0; c < 3; ++c) dsum += std::fabs(h[(size_t)stencil_k(13, c, c) * nnL + i]);
-        shift = (shift == 0.0 ? 1e-12 : shift * 1e3) * std::max(dsum / n, 1e-300);
-      }
-      TP3D_CHECK(cudaMemsetAsync(s->cdense, 0, (size_t)n * n * sizeof(double), st));
-      dense_from_stencil_kernel<<<s->grid_blocks(s->grids[L].nnode()), 256, 0, st>>>(s->grids[L], s->A64[L],
-                                                                                      s->fix[L], s->cdense);
-      count_launch();
-      if (shift > 0.0) {
-        dense_shift_kernel<<<s->grid_blocks(n), 256, 0, st>>>(n, s->cdense, shift);
-        count_launch();
-      }
-      if (n <= kGjRegMaxN) {
-        dense_gj_inverse_reg_kernel<<<1, 512, 0, st>>>(n, s->cdense, s->cinv64, s->cstatus);
-        count_launch();
-      } else {
-        const size_t smem = 2 * (size_t)n * sizeof(double);
-        if (smem > 48 * 1024)
-          TP3D_CHECK(cudaFuncSetAttribute(dense_gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-        dense_gj_inverse_kernel<<<1, 1024, smem, st>>>(n, s->cdense, s->cinv64, 0, s->cstatus);
-        count_launch();
-      }
-      TP3D_CHECK_LAUNCH();
-      TP3D_CHECK(cudaMemcpyAsync(&status, s->cstatus, sizeof(int), cudaMemcpyDeviceToHost, st));
-      TP3D_CHECK(cudaStreamSynchronize(st));
-    }
-    if (status != 0) {  // fall back to the inverse diagonal of the coarsest operator
-      s->coarse_fallback = true;
-      TP3D_CHECK(cudaMemsetAsync(s->cdense, 0, (size_t)n * n * sizeof(double), st));
-      dense_from_stencil_kernel<<<s->grid_blocks(s->grids[L].nnode()), 256, 0, st>>>(s->grids[L], s->A64[L],
-                                                                                      s->fix[L], s->cdense);
-      dense_diag_inverse_kernel<<<s->grid_blocks((long long)n * n), 256, 0, st>>>(n, s->cdense, s->cinv64);
-      count_launch();
-      count_launch();
-    }
-    if (mixed) {
-      convert_kernel<double, float><<<s->grid_blocks((long long)n * n), 256, 0, st>>>((long long)n * n, s->cinv64,
-                                                                                      s->cinv32);
-      count_launch();
-    }
-  } else if (s->nlev > 1) {
-    s->coarse_fallback = false;
-  }
+  // the solve waits for the coarsest inverse; its status (shifted attempts,
+  // diagonal fallback) stays on the device until tp3d_solver_stats reads it
+  if (s->nlev > 1) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
   TP3D_CHECK_LAUNCH();
   s->have_density = true;
   return s->leave();
@@ -1816,15 +1767,22 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
     cudaStreamSynchronize(s->st);
     for (int L = 0; L < s->nlev; ++L) cudaMemcpy(&lam[L], s->coef[L] + 1, sizeof(double), cudaMemcpyDeviceToHost);
   }
+  int gj_status = 0;
+  if (s->have_density && s->nlev > 1) {
+    cudaStreamSynchronize(s->st_side);
+    cudaMemcpy(&gj_status, s->cstatus, sizeof(int), cudaMemcpyDeviceToHost);
+  }
+  const bool coarse_fallback = gj_status == kGjFallback;
   std::vector<double> v = {(double)s->nlev, (double)s->last_iters, (double)s->last_updates, s->last_relres,
                            (double)s->last_restarts, (double)s->cn, (double)s->tile.TY, (double)s->tile.TX,
-                           (double)s->tile.ZC, s->coarse_fallback ? 1.0 : 0.0, lam.empty() ? 0.0 : lam[0],
+                           (double)s->tile.ZC, coarse_fallback ? 1.0 : 0.0, lam.empty() ? 0.0 : lam[0],
                            s->last_floor ? 1.0 : 0.0, s->last_fallback ? 1.0 : 0.0,
                            s->use_wht64 ? 1.0 + s->wt64.variant : 0.0,
                            s->mixed ? (s->use_wht32 ? 1.0 + s->wt32.variant : 0.0) : -1.0,
                            (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0,
                            s->pdl ? (double)s->o.pdl : 0.0,
-                           (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; })};
+                           (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; }),
+                           (double)gj_status};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

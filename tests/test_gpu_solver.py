@@ -317,6 +317,32 @@ def test_iteration_cap_raises_runtime_error(P):
     s.close()
 
 
+# The coarsest dense inverse handles a failed elimination on the device: an
+# operator with negative moduli (negative densities, E = -1) has a negative
+# first pivot, every shifted attempt fails too, and the inverse falls back to
+# the inverse diagonal (zero where the diagonal is not positive); a normal
+# operator takes the first attempt.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_coarsest_inverse_falls_back_on_the_device(P, prec):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 16, 8, 8
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=9, lo=0.1)
+    s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, smoother=1)
+    s.set_density(to_flat(rho), 3.0)
+    st = s.stats()
+    assert st["coarsest_status"] == 0 and st["coarse_fallback"] == 0, st
+    s.set_density(to_flat(-np.ones_like(rho)), 3.0)
+    st = s.stats()
+    assert st["coarsest_status"] == 4 and st["coarse_fallback"] == 1, st
+    s.set_density(to_flat(rho), 3.0)  # and back
+    st = s.stats()
+    assert st["coarsest_status"] == 0 and st["coarse_fallback"] == 0, st
+    s.close()
+
+
 def test_nonfinite_density_reports_an_error_not_a_hang(P):
     from pytopo3d_b200._tensors import to_flat
     from pytopo3d_b200.solver import HexSolver
