@@ -538,18 +538,31 @@ __global__ void __launch_bounds__(512, 1) dense_gj_inverse_reg_kernel(int n, con
       double g[C];
 #pragma unroll
       for (int c = 0; c < C; ++c) g[c] = rowk[buf][l + 32 * c];
+      // every entry: a_ij -= (a_ik / a_kk) a_kj (one FMA each); row k and
+      // column k are then overwritten by their owners
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const bool rk = (w + 16 * r) == k;
         const double f = colk[buf][w + 16 * r] * pk;
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-          const bool ck = (l + 32 * c) == k;
-          double v = a[r][c] - f * g[c];
-          if (ck) v = -f;
-          if (rk) v = ck ? pk : g[c] * pk;
-          a[r][c] = v;
-        }
+        for (int c = 0; c < C; ++c) a[r][c] = a[r][c] - f * g[c];
+      }
+      if (w == (k & 15)) {  // row k: a_kj / a_kk
+        const int kr = k >> 4;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          if (r == kr) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) a[r][c] = g[c] * pk;
+          }
+      }
+      if (l == (k & 31)) {  // column k: -a_ik / a_kk, and 1 / a_kk on the diagonal
+        const int kc = k >> 5;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+          if (c == kc) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[r][c] = (w + 16 * r == k) ? pk : -(colk[buf][w + 16 * r] * pk);
+          }
       }
     }
     __syncthreads();  // the last step's buffers are read before the next attempt writes them

@@ -40,6 +40,7 @@ inline void count_launch() {
 }
 
 constexpr int kMaxPartials = 1 << 16;
+constexpr int kSpectraPartials = 4096;  // per level at set-up: two reductions of at most 2048 blocks
 constexpr int kPdlCoarse = 1, kPdlFine = 2;  // tp3d_solver_opts::pdl bits
 
 template <typename T>
@@ -213,7 +214,6 @@ struct tp3d_solver {
   double* E64 = nullptr;
   float* E32 = nullptr;
   __nv_bfloat16* rho16 = nullptr;
-  double* pw[2] = {nullptr, nullptr};  // power-iteration work vectors (fine size)
   std::vector<double*> pv;              // per-level normalised dominant vectors (warm starts)
   bool have_spectra = false;
 
@@ -238,6 +238,8 @@ struct tp3d_solver {
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
   cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
+  std::vector<cudaStream_t> st_pow;   // one per smoothed level: its power iteration
+  std::vector<cudaEvent_t> ev_pow_in, ev_pow_out;
   cudaEvent_t ev_side_in = nullptr, ev_side_out = nullptr, ev_side_elem = nullptr;
   unsigned int* loop_passes = nullptr;
   unsigned int* loop_pass_host = nullptr;
@@ -279,6 +281,9 @@ struct tp3d_solver {
     if (loop_pass_host) cudaFreeHost(loop_pass_host);
     if (st_branch) cudaStreamDestroy(st_branch);
     if (st_side) cudaStreamDestroy(st_side);
+    for (cudaStream_t p : st_pow) if (p) cudaStreamDestroy(p);
+    for (cudaEvent_t e : ev_pow_in) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_pow_out) if (e) cudaEventDestroy(e);
     if (ev_side_in) cudaEventDestroy(ev_side_in);
     if (ev_side_out) cudaEventDestroy(ev_side_out);
     if (ev_side_elem) cudaEventDestroy(ev_side_elem);
@@ -1383,9 +1388,14 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   s->fin_count = s->alloc<unsigned int>(1);
   if (s->fin_count) cudaMemset(s->fin_count, 0, sizeof(unsigned int));
   s->loop_passes = s->alloc<unsigned int>(1);
+  // The side stream (element chain, coarsest stencil and inverse: the longest
+  // chain of the set-up) gets the highest priority, so that its blocks are
+  // scheduled ahead of the level builds and power iterations running beside it.
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   if (cudaMallocHost(&s->loop_pass_host, sizeof(unsigned int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->st_branch, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&s->st_side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_side_in, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_side_out, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_side_elem, cudaEventDisableTiming) != cudaSuccess)
@@ -1431,6 +1441,15 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   }
   s->A64.assign(s->nlev, nullptr);
   s->S16.assign(s->nlev, nullptr);
+  s->st_pow.assign(s->nlev, nullptr);
+  s->ev_pow_in.assign(s->nlev, nullptr);
+  s->ev_pow_out.assign(s->nlev, nullptr);
+  if ((long long)s->nlev * kSpectraPartials > kMaxPartials) return fail(TP3D_ERR_ARG, "too many levels");
+  for (int L = 0; L < s->nlev; ++L)
+    if (cudaStreamCreateWithFlags(&s->st_pow[L], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_pow_in[L], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_pow_out[L], cudaEventDisableTiming) != cudaSuccess)
+      return fail(TP3D_ERR_CUDA, "solver setup failed");
   s->L64.resize(s->nlev);
   if (mixed) s->L32.resize(s->nlev);
   for (int L = 0; L < s->nlev; ++L) {
@@ -1467,8 +1486,6 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   }
   const long long ndof = 3 * s->g.nnode();
   for (int L = 0; L < s->nlev; ++L) s->pv.push_back(s->alloc<double>(3 * s->grids[L].nnode()));
-  s->pw[0] = s->alloc<double>(ndof);
-  s->pw[1] = s->alloc<double>(ndof);
   s->u64 = s->alloc<double>(ndof);
   if (!mixed) {
     s->K64.u = s->u64;
@@ -1497,58 +1514,77 @@ extern "C" int tp3d_solver_destroy(tp3d_solver* s) {
   return TP3D_OK;
 }
 
-// lambda_max(Dinv A) per level by power iteration, then the Chebyshev
-// coefficients; all on the device.  The operators are those of the solve's
-// own precision (FP32 in the mixed form: two digits of lambda_max suffice).
-// The first call starts from a pseudo-random vector; later calls start from
-// the previous (normalised) dominant vector, which tracks the slowly changing
-// design in fewer steps.
+// lambda_max(Dinv A) of level L by power iteration, then its Chebyshev
+// coefficients; all on the device, on the stream `ps` (each level has its own,
+// so the levels' iterations, latency-bound on the small levels, overlap one
+// another and the builds of the levels after them).  The operators are those of
+// the solve's own precision (FP32 in the mixed form: two digits of lambda_max
+// suffice).  The first set-up starts from a pseudo-random vector; later ones
+// from the previous (normalised) dominant vector, which tracks the slowly
+// changing design in fewer steps.
+
 template <typename T>
-static int estimate_spectra(tp3d_solver* s) {
-  cudaStream_t st = s->st;
+static int spectra_level(tp3d_solver* s, int L, cudaStream_t ps) {
   const bool warm = s->have_spectra;
   const int N = warm ? std::max(3, s->o.power_iterations / 3) : s->o.power_iterations;
-  for (int L = 0; L < s->nlev - (s->nlev > 1 ? 1 : 0); ++L) {
-    const long long nn = s->grids[L].nnode(), ndof = 3 * nn;
-    const int nb = s->grid_blocks(ndof);
-    auto& lv = s->levels<T>()[L];
-    T* w[2];
+  const long long nn = s->grids[L].nnode(), ndof = 3 * nn;
+  const int nb = s->grid_blocks(ndof);
+  auto& lv = s->levels<T>()[L];
+  T* w[2] = {lv.x[0], lv.x[1]};
+  double* pa = s->partials + (size_t)L * kSpectraPartials;
+  double* pb = pa + kSpectraPartials / 2;
+  std::swap(s->st, ps);  // apply_level launches on s->st
+  cudaStream_t st = s->st;
+  int rc = TP3D_OK;
+  if (warm) {
     if constexpr (sizeof(T) == 8) {
-      w[0] = s->pw[0];
-      w[1] = s->pw[1];
+      rc = cuda_status(cudaMemcpyAsync(w[0], s->pv[L], ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
     } else {
-      w[0] = lv.x[0];
-      w[1] = lv.x[1];
-    }
-    if (warm) {
-      if constexpr (sizeof(T) == 8) {
-        TP3D_CHECK(cudaMemcpyAsync(w[0], s->pv[L], ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      } else {
-        convert_kernel<double, T><<<nb, 256, 0, st>>>(ndof, s->pv[L], w[0]);
-        count_launch();
-      }
-    } else {
-      random_vector_kernel<T><<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->fix[L], w[0]);
+      convert_kernel<double, T><<<nb, 256, 0, st>>>(ndof, s->pv[L], w[0]);
       count_launch();
     }
-    int cur = 0;
-    for (int k = 0; k < N; ++k) {
-      OpIO<T> io;
-      io.u = w[cur];
-      io.out = w[1 - cur];
-      io.dinv = lv.dinv;
-      if (int rc = s->apply_level<T, kModeDinvApply>(L, io)) return rc;
-      cur = 1 - cur;
-    }
-    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], w[cur], s->partials, nullptr, nullptr);
-    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[1 - cur], w[1 - cur], s->partials + kMaxPartials / 2, nullptr,
-                                      nullptr);
-    cheb_setup_kernel<<<1, 256, 0, st>>>(s->partials, nb, s->partials + kMaxPartials / 2, nb, s->o.cheb_ratio,
-                                         1.1, s->coef[L]);
+  } else {
+    random_vector_kernel<T><<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->fix[L], w[0]);
+    count_launch();
+  }
+  int cur = 0;
+  for (int k = 0; k < N && rc == TP3D_OK; ++k) {
+    OpIO<T> io;
+    io.u = w[cur];
+    io.out = w[1 - cur];
+    io.dinv = lv.dinv;
+    rc = s->apply_level<T, kModeDinvApply>(L, io);
+    cur = 1 - cur;
+  }
+  if (rc == TP3D_OK) {
+    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], w[cur], pa, nullptr, nullptr);
+    dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[1 - cur], w[1 - cur], pb, nullptr, nullptr);
+    cheb_setup_kernel<<<1, 256, 0, st>>>(pa, nb, pb, nb, s->o.cheb_ratio, 1.1, s->coef[L]);
     scale_copy_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], s->coef[L] + kCoefLen - 1, s->pv[L]);
     for (int i = 0; i < 4; ++i) count_launch();
-    TP3D_CHECK_LAUNCH();
+    rc = cuda_status(cudaGetLastError());
   }
+  std::swap(s->st, ps);
+  return rc;
+}
+
+// Level L's power iteration on its own stream, after what the solver's stream
+// has queued so far (level L's operator); the solver's stream joins all of them
+// at the end of the set-up (join_spectra).
+static int fork_spectra(tp3d_solver* s, int L) {
+  if (s->o.smoother == 1 || L >= s->nlev - 1 + (s->nlev == 1 ? 1 : 0)) return TP3D_OK;
+  cudaStream_t ps = s->st_pow[L];
+  TP3D_CHECK(cudaEventRecord(s->ev_pow_in[L], s->st));
+  TP3D_CHECK(cudaStreamWaitEvent(ps, s->ev_pow_in[L], 0));
+  if (int rc = s->mixed ? spectra_level<float>(s, L, ps) : spectra_level<double>(s, L, ps)) return rc;
+  TP3D_CHECK(cudaEventRecord(s->ev_pow_out[L], ps));
+  return TP3D_OK;
+}
+
+static int join_spectra(tp3d_solver* s) {
+  if (s->o.smoother == 1) return TP3D_OK;
+  for (int L = 0; L < s->nlev - 1 + (s->nlev == 1 ? 1 : 0); ++L)
+    TP3D_CHECK(cudaStreamWaitEvent(s->st, s->ev_pow_out[L], 0));
   s->have_spectra = true;
   return TP3D_OK;
 }
@@ -1581,6 +1617,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       if (int rc = s->choose_fine_form<float>()) return rc;
     s->fine_chosen = true;
   }
+  if (int rc = fork_spectra(s, 0)) return rc;
   // The coarsest inverse (one block) runs on a side stream while the level
   // builds and the power iterations use the rest of the GPU; its status is read
   // after both.
@@ -1677,6 +1714,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       s->pack_level<double>(L, s->L64[L].A);
     }
     TP3D_CHECK_LAUNCH();
+    if (int rc = fork_spectra(s, L)) return rc;
   }
   if (s->nlev > 1 && !elem_chain) {
     TP3D_CHECK(cudaEventRecord(s->ev_side_in, st));
@@ -1684,8 +1722,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     if (int rc = coarsest_gj(s->st_side)) return rc;
     TP3D_CHECK(cudaEventRecord(s->ev_side_out, s->st_side));
   }
-  if (s->o.smoother != 1)
-    if (int rc = mixed ? estimate_spectra<float>(s) : estimate_spectra<double>(s)) return rc;
+  if (int rc = join_spectra(s)) return rc;
   // the solve waits for the coarsest inverse; its status (shifted attempts,
   // diagonal fallback) stays on the device until tp3d_solver_stats reads it
   if (s->nlev > 1) TP3D_CHECK(cudaStreamWaitEvent(st, s->ev_side_out, 0));
