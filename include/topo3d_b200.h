@@ -188,6 +188,9 @@ typedef struct tp3d_solver_opts {
   int split_dofs;       /* coarse levels with at most this many DOFs apply their stencil with four
                            threads per DOF (more loads in flight on levels too small to fill the
                            GPU); larger levels one thread per DOF */
+  int deep_cta;         /* mixed form, 1 (default): the last smoothed level and the coarsest solve run
+                           as one thread block with the level's operator in shared memory (when it
+                           fits), instead of one launch per smoothing step and grid transfer */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -232,7 +235,8 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * coarse cycle (0 none), 1 when the CG loop runs on the device (one graph launch per
  * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none),
  * the number of levels whose stencils are held in bf16, the coarsest inverse's status (0 first
- * attempt, 1-3 attempts with a raised diagonal, 4 diagonal fallback).  Returns the count written. */
+ * attempt, 1-3 attempts with a raised diagonal, 4 diagonal fallback), the level run as one block
+ * with the coarsest solve (0 none).  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

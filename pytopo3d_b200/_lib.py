@@ -56,6 +56,7 @@ class SolverOpts(C.Structure):
         ("pdl", i32),
         ("coarse_bf16", i32),
         ("split_dofs", i32),
+        ("deep_cta", i32),
     ]
 
 

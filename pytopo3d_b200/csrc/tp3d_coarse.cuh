@@ -65,7 +65,7 @@ __device__ __forceinline__ void cycle_smooth_dof(const CycleLevel<T>& lv, int cu
   io.step = s;
   io.omega = omega;
   const int n = i / 3, c = i - 3 * n;
-  const T kv = stencil_row<T>(lv.g, lv.S, io.u, i);
+  const T kv = stencil_row<T, T, LdL2>(lv.g, lv.S, io.u, i);
   const bool fx = (lv.fix[n] >> c) & 1;
   double part = 0.0;
   op_epilogue<T, MODE>(io, i, fx, kv, fx ? T(0) : io.u[i], epi_load<T, MODE>(io, i), part);
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) coarse_cycle_kernel(const __grid_constant
     for (int i = tid; i < ndof; i += nth) {
       const int n = i / 3, c = i - 3 * n;
       const bool fx = (lv.fix[n] >> c) & 1;
-      lv.r[i] = fx ? T(0) : lv.b[i] - stencil_row<T>(lv.g, lv.S, lv.x[cur], i);
+      lv.r[i] = fx ? T(0) : lv.b[i] - stencil_row<T, T, LdL2>(lv.g, lv.S, lv.x[cur], i);
     }
     if (!sync()) return;
     const CycleLevel<T>& lc = p.lv[L + 1];
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) coarse_cycle_kernel(const __grid_constant
     const bool smooth_next = L + 1 < p.Lc;
     for (int n = tid; n < nnc; n += nth) {
       const int Iy = n % CY, r = n / CY;
-      restrict_node<T>(lv.g, lc.g, lv.r, lc.fix, lc.b, r % CX, Iy, r / CX);
+      restrict_node<T, LdL2>(lv.g, lc.g, lv.r, lc.fix, lc.b, r % CX, Iy, r / CX);
       if (smooth_next)
         for (int c = 0; c < 3; ++c) smooth_zero(lc, 3 * n + c);
     }
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256) coarse_cycle_kernel(const __grid_constant
     const int nnf = (int)lv.g.nnode();
     for (int n = tid; n < nnf; n += nth) {
       const int iy = n % FY, r = n / FY;
-      prolong_node<T>(lv.g, lc.g, xc, lv.fix, lv.x[cur], r % FX, iy, r / FX);
+      prolong_node<T, LdL2>(lv.g, lc.g, xc, lv.fix, lv.x[cur], r % FX, iy, r / FX);
     }
     if (!sync()) return;
     for (int s = 0; s < p.post; ++s) {

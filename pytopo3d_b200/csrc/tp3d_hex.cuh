@@ -263,10 +263,26 @@ struct StencilParams {
   OpIO<T> io;
 };
 
-template <typename T>
-__device__ __forceinline__ T ld_coef(const T* p) { return __ldg(p); }
-template <typename T>
-__device__ __forceinline__ T ld_coef(const __nv_bfloat16* p) { return (T)__bfloat162float(__ldg(p)); }
+// Load policies of the operator device functions: LdRO through the read-only
+// path (data no kernel writes during the launch), LdL2 at L2 (data written
+// earlier in the same launch by other blocks), LdPlain for shared memory.
+struct LdRO {
+  template <typename V>
+  __device__ __forceinline__ V operator()(const V* p) const { return __ldg(p); }
+};
+struct LdL2 {
+  template <typename V>
+  __device__ __forceinline__ V operator()(const V* p) const { return __ldcg(p); }
+};
+struct LdPlain {
+  template <typename V>
+  __device__ __forceinline__ V operator()(const V* p) const { return *p; }
+};
+
+template <typename T, class Ld = LdRO>
+__device__ __forceinline__ T ld_coef(const T* p) { return Ld()(p); }
+template <typename T, class Ld = LdRO>
+__device__ __forceinline__ T ld_coef(const __nv_bfloat16* p) { return (T)__bfloat162float(Ld()(p)); }
 
 // One DOF per thread: 81 coalesced coefficient loads and 81 neighbour loads,
 // all independent (offsets past the grid are clamped to the node itself and
@@ -274,8 +290,9 @@ __device__ __forceinline__ T ld_coef(const __nv_bfloat16* p) { return (T)__bfloa
 // levels hold far fewer than 2^31 DOFs: 32-bit index arithmetic.
 // Row i of the packed stencil times u (K u at DOF i; fixed rows and columns are
 // zero in the packed layout).
-template <typename T, typename TS = T>
+template <typename T, typename TS = T, class Ld = LdRO>
 __device__ __forceinline__ T stencil_row(const Grid& g, const TS* __restrict__ S, const T* __restrict__ u, int i) {
+  const Ld ld;
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const int NXY = NX * NY;
   const int ndof = 3 * NXY * NZ;
@@ -297,9 +314,9 @@ __device__ __forceinline__ T stencil_row(const Grid& g, const TS* __restrict__ S
         const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
         const int m3 = 3 * (n + oz + ox + oy);
         const TS* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
-        kv = fma(ld_coef<T>(s), __ldg(&u[m3]), kv);
-        kv = fma(ld_coef<T>(s + ndof), __ldg(&u[m3 + 1]), kv);
-        kv = fma(ld_coef<T>(s + 2 * (size_t)ndof), __ldg(&u[m3 + 2]), kv);
+        kv = fma(ld_coef<T, Ld>(s), ld(&u[m3]), kv);
+        kv = fma(ld_coef<T, Ld>(s + ndof), ld(&u[m3 + 1]), kv);
+        kv = fma(ld_coef<T, Ld>(s + 2 * (size_t)ndof), ld(&u[m3 + 2]), kv);
       }
     }
   }
@@ -441,9 +458,10 @@ inline dim3 plane_grid(int nxy, int nz) { return dim3((unsigned)((nxy + 255) / 2
 // b_c[I] = sum_i P[i,I] r_f[i], 0 on fixed coarse DOFs.  The 27 fine
 // neighbours are read unconditionally (offsets past the fine grid are clamped
 // and weighted 0), so the loads are independent.  Grid: plane_grid(CX*CY, CZ).
-template <typename T>
+template <typename T, class Ld = LdRO>
 __device__ __forceinline__ void restrict_node(const Grid& gf, const Grid& gc, const T* __restrict__ rf,
                                               const uint8_t* __restrict__ fixc, T* bc, int Ix, int Iy, int Iz) {
+  const Ld ld;
   const int FX = gf.nx + 1, FY = gf.ny + 1, FZ = gf.nz + 1;
   const int CX = gc.nx + 1, CY = gc.ny + 1;
   const int FXY = FX * FY;
@@ -462,9 +480,9 @@ __device__ __forceinline__ void restrict_node(const Grid& gf, const Grid& gc, co
         const bool v = vz && vx && y >= 0 && y < FY;
         const T w = v ? T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0)) : T(0);
         const T* src = rf + 3 * (v ? y + FY * x + FXY * z : 0);
-        s0 = fma(w, __ldg(src), s0);
-        s1 = fma(w, __ldg(src + 1), s1);
-        s2 = fma(w, __ldg(src + 2), s2);
+        s0 = fma(w, ld(src), s0);
+        s1 = fma(w, ld(src + 1), s1);
+        s2 = fma(w, ld(src + 2), s2);
       }
     }
   }
@@ -515,9 +533,10 @@ __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T
 // x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.  A fine node takes 1, 2, 4
 // or 8 coarse nodes (weights 1 or 1/2 per axis), read as a fixed 2x2x2 block
 // with zero weights for the absent ones.  Grid: plane_grid(FX*FY, FZ).
-template <typename T>
+template <typename T, class Ld = LdRO>
 __device__ __forceinline__ void prolong_node(const Grid& gf, const Grid& gc, const T* __restrict__ xc,
                                              const uint8_t* __restrict__ fixf, T* xf, int ix, int iy, int iz) {
+  const Ld ld;
   const int FX = gf.nx + 1, FY = gf.ny + 1;
   const int CX = gc.nx + 1, CY = gc.ny + 1;
   const long long n = iy + (long long)FY * (ix + (long long)FX * iz);
@@ -539,9 +558,9 @@ __device__ __forceinline__ void prolong_node(const Grid& gf, const Grid& gc, con
         const T wy = oy ? h : (e ? T(0) : T(1));
         const T w = wz * wx * wy;
         const T* src = xc + 3 * (base + (e & oy) + CY * (b & ox) + CXY * (a & oz));
-        s0 = fma(w, __ldg(src), s0);
-        s1 = fma(w, __ldg(src + 1), s1);
-        s2 = fma(w, __ldg(src + 2), s2);
+        s0 = fma(w, ld(src), s0);
+        s1 = fma(w, ld(src + 1), s1);
+        s2 = fma(w, ld(src + 2), s2);
       }
     }
   }

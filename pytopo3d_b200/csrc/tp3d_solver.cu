@@ -26,6 +26,7 @@
 #include "tp3d_fine.cuh"
 #include "tp3d_fine_wht.cuh"
 #include "tp3d_coarse.cuh"
+#include "tp3d_deep.cuh"
 #include "tp3d_pcg.cuh"
 
 namespace tp3d {
@@ -257,6 +258,10 @@ struct tp3d_solver {
   // coarse end of the V-cycle as one cooperative launch from level cyc_L0
   // (0: off); grid barrier state
   int cyc_L0 = 0;
+  // the last smoothed level and the coarsest solve in one block (mixed form;
+  // 0 none), and that block's shared memory
+  int deep_L = 0;
+  size_t deep_smem = 0;
   int cyc_blocks64 = 0, cyc_blocks32 = 0;
   unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
@@ -659,6 +664,45 @@ struct tp3d_solver {
     return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.post_sweeps;
   }
 
+  // Level L (the last smoothed level) and the coarsest solve as one block
+  // (deep_cycle_kernel); the restriction that produced b took the first
+  // smoothing step.  Returns the buffer holding level L's iterate.
+  float* deep_cycle(int L, const float* b, const int* done, int* rc) {
+    auto& lv = L32[L];
+    auto fill = [&](auto& p) {
+      p.g = grids[L];
+      p.gc = grids[L + 1];
+      p.fix = fix[L];
+      p.fixc = fix[L + 1];
+      p.dinv = lv.dinv;
+      p.coef = coef[L];
+      p.inv = cinv32;
+      p.cn = cn;
+      p.b = b;
+      p.x0 = lv.x[0];
+      p.d0 = o.smoother != 1 ? lv.d : nullptr;
+      p.xout = lv.x[0];
+      p.pre = pre_sweeps(L);
+      p.post = post_sweeps(L);
+      p.cheb = o.smoother != 1;
+      p.omega = (float)o.omega;
+      p.done = done;
+    };
+    if (S16[L]) {
+      DeepParams<float, __nv_bfloat16> p;
+      fill(p);
+      p.S = S16[L];
+      launch(kPdlCoarse, deep_cycle_kernel<float, __nv_bfloat16>, dim3(1), dim3(kDeepThreads), deep_smem, p);
+    } else {
+      DeepParams<float, float> p;
+      fill(p);
+      p.S = lv.A;
+      launch(kPdlCoarse, deep_cycle_kernel<float, float>, dim3(1), dim3(kDeepThreads), deep_smem, p);
+    }
+    if (cudaGetLastError() != cudaSuccess) *rc = TP3D_ERR_CUDA;
+    return lv.x[0];
+  }
+
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
   // zero_done: the first smoothing step from zero already ran (fused into the
@@ -686,6 +730,8 @@ struct tp3d_solver {
       return lv.x[0];
     }
     if (L == cyc_L0 && cyc_L0 > 0) return coarse_cycle<T>(L, b, rc);
+    if constexpr (sizeof(T) == 4)
+      if (L == deep_L && deep_L > 0 && zero_done) return deep_cycle(L, b, done, rc);
     const bool cheb = o.smoother != 1;
     int cur = 0;
     if (!zero_done) {
@@ -1295,6 +1341,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->pdl = 2;
   o->coarse_bf16 = 99;
   o->split_dofs = 16384;
+  o->deep_cta = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1502,6 +1549,25 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   }
   for (void* p : s->allocs)
     if (!p) return fail(TP3D_ERR_CUDA, "allocation failed");
+  // the last smoothed level in one block when its operator fits in shared memory
+  if (mixed && o.deep_cta && s->nlev >= 3 && s->cyc_L0 == 0) {
+    const int L = s->nlev - 2;
+    const bool b16 = s->S16[L] != nullptr;
+    const long long nn = s->grids[L].nnode(), nnc = s->grids[L + 1].nnode();
+    const size_t smem = b16 ? deep_smem_bytes<float, __nv_bfloat16>(nn, nnc) : deep_smem_bytes<float, float>(nn, nnc);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const cudaError_t e = b16 ? cudaFuncSetAttribute(deep_cycle_kernel<float, __nv_bfloat16>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                              : cudaFuncSetAttribute(deep_cycle_kernel<float, float>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem <= (size_t)optin && e == cudaSuccess) {
+      s->deep_L = L;
+      s->deep_smem = smem;
+    }
+    cudaGetLastError();
+  }
   if (cudaStreamSynchronize(s->st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
     return fail(TP3D_ERR_CUDA, "setup failed");
   *out = s;
@@ -1819,7 +1885,7 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0,
                            s->pdl ? (double)s->o.pdl : 0.0,
                            (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; }),
-                           (double)gj_status};
+                           (double)gj_status, (double)s->deep_L};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -121,7 +121,7 @@ class HexSolver:
         keys = ["levels", "iterations", "reliable_updates", "relres", "restarts", "coarsest_dofs",
                 "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor",
                 "fp64_fallback", "fine_form_fp64", "fine_form_fp32", "fused_cycle_level", "device_loop",
-                "pdl", "coarse_bf16", "coarsest_status"]
+                "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
 
 

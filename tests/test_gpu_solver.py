@@ -206,6 +206,41 @@ def test_split_stencil_matches_one_thread_per_dof(P, dims, prec):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=tol * np.abs(Us[0]).max())
 
 
+# The last smoothed level and the coarsest solve as one block (mixed form)
+# compute what the per-phase launches compute (the stencil rows summed in one
+# thread's order rather than four lanes'): same iterations within one or 2%,
+# same solution to the mixed form's rounding.  The block holds the level's
+# operator in shared memory, so it is used when that fits: a last smoothed
+# level of at most about 400 nodes with bf16 stencils (64x32x32: 9x5x5 nodes;
+# 40x20x20: 11x6x6; 16x8x8: 9x5x5), not for 48x24x24 (13x7x7), and not with
+# damped Jacobi, whose levels keep FP32 stencils (twice the bytes).
+@pytest.mark.parametrize("smoother", [0, 1])
+@pytest.mark.parametrize("dims,fits", [((64, 32, 32), True), ((40, 20, 20), True), ((16, 8, 8), True),
+                                       ((48, 24, 24), False)])
+def test_deep_block_cycle_matches_per_phase_launches(P, dims, fits, smoother):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=8, lo=0.3 if smoother else 0.0)
+    if not smoother:
+        rho[rho < 0.25] = 0.0
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    its, Us = [], []
+    for deep in (0, 1):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", deep_cta=deep, smoother=smoother, fine_operator=3)
+        s.set_density(to_flat(rho), 3.0)
+        st = s.stats()
+        assert st["deep_cta_level"] == (st["levels"] - 2 if deep and fits and not smoother else 0), st
+        U = s.solve(F)
+        its.append(s.last_iterations)
+        Us.append(U.cpu().numpy())
+        s.close()
+    assert abs(its[0] - its[1]) <= max(1, 0.02 * its[0]), its
+    np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
+
+
 # Programmatic dependent launch only changes when a kernel may be scheduled,
 # never what it computes or in which order the kernels' writes land: every
 # mask gives bit-identical iterations and solutions, with the device loop.
