@@ -18,6 +18,7 @@ time).
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import subprocess
@@ -65,7 +66,12 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    The sampler is started before the warm-up (nvidia-smi takes a moment to
+    start); ``timed()`` brackets the timed region and only samples taken inside
+    it (or, for a region shorter than the sampling interval, the one nearest to
+    it) enter the summary."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -75,11 +81,12 @@ class ClockSampler:
         self.idx = gpu_index
         self.rows = []
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -89,7 +96,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            self.rows.append((time.perf_counter(), [c.strip() for c in line.split(",")]))
+
+    @contextlib.contextmanager
+    def timed(self):
+        t0 = time.perf_counter()
+        yield
+        self.window = (t0, time.perf_counter())
 
     def __exit__(self, *a):
         if self.proc:
@@ -100,11 +113,18 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = list(self.rows)
+        if self.window and rows:
+            t0, t1 = self.window
+            inside = [r for t, r in rows if t0 <= t <= t1 + 0.05]
+            rows = inside or [min(rows, key=lambda tr: abs(tr[0] - 0.5 * (t0 + t1)))[1]]
+        else:
+            rows = [r for _, r in rows]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        for r in rows:
             if len(r) >= 9:
                 for n, v in zip(names, r[5:9]):
                     if v.lower().startswith("active"):
@@ -297,14 +317,18 @@ def main():
     results = {}
     for prec in ([args.precision] + [p for p in ("fp64", "mixed") if p != args.precision]):
         loop = make_loop(prec)
-        for _ in range(W):
-            loop.step()
-        torch.cuda.synchronize()
         if prec == args.precision:
             with ClockSampler(local) as clk:
-                ms, cg, launches, c = time_device_steps(loop, args.steps, dist)
+                for _ in range(W):
+                    loop.step()
+                torch.cuda.synchronize()
+                with clk.timed():
+                    ms, cg, launches, c = time_device_steps(loop, args.steps, dist)
             clocks = clk.summary()
         else:
+            for _ in range(W):
+                loop.step()
+            torch.cuda.synchronize()
             ms, cg, launches, c = time_device_steps(loop, max(3, args.steps // 4), dist)
         steps = args.steps if prec == args.precision else max(3, args.steps // 4)
         ms = max_over_ranks(ms, dist)
