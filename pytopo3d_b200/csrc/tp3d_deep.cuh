@@ -6,12 +6,15 @@
 // matrix-vector product, launched separately, cost a kernel's launch, ramp
 // and drain for microseconds of work.  Here one block of 1024 threads runs the
 // level's whole cycle with block barriers between the phases: it stages the
-// level's packed stencil (bf16 or FP32), diagonal, masks and vectors in shared
-// memory once, smooths, restricts the residual, multiplies by the coarsest
-// inverse (read from global memory once), prolongs and smooths again, and
-// writes the level's iterate back.  Every phase calls the same per-DOF and
-// per-node device functions as the separate kernels, with plain loads from
-// shared memory, so it computes what they compute.
+// level's packed stencil (bf16 or FP32), the coarsest inverse (when it fits),
+// diagonal, masks and vectors in shared memory once (asynchronous 16-byte
+// copies, all in flight together), smooths, restricts the residual,
+// multiplies by the coarsest inverse, prolongs and smooths again, and writes
+// the level's iterate back.  Every phase calls the same per-node device
+// functions and epilogues as the separate kernels, with plain loads from
+// shared memory; a stencil row is summed in three partial sums (one per
+// z-plane of neighbours) to shorten its dependent chain, so rows round
+// differently from the separate kernels' single sum.
 #pragma once
 
 #include "tp3d_hex.cuh"
@@ -30,6 +33,7 @@ struct DeepParams {
   const double* coef = nullptr;  // Chebyshev coefficients of the level
   const T* inv = nullptr;        // coarsest inverse, cn x cn row-major
   int cn = 0;
+  int inv_smem = 0;              // 1: the inverse is staged in shared memory
   const T* b = nullptr;          // the level's right-hand side
   const T* x0 = nullptr;         // its first smoothing step (written by the restriction)
   const T* d0 = nullptr;         // and that step's Chebyshev direction
@@ -42,13 +46,63 @@ struct DeepParams {
 
 // Shared-memory bytes of the block for a level of `nn` nodes and a coarsest
 // level of `nnc` nodes: stencil (81 coefficients per DOF), six level vectors
-// (x[2], b, d, dinv, r), two coarsest vectors, node masks; 16-byte aligned parts.
+// (x[2], b, d, dinv, r), two coarsest vectors, node masks, and with inv_smem
+// the coarsest inverse; 16-byte aligned parts.
 template <typename T, typename TS>
-__host__ __device__ constexpr size_t deep_smem_bytes(long long nn, long long nnc) {
+__host__ __device__ constexpr size_t deep_smem_bytes(long long nn, long long nnc, bool inv_smem) {
   const size_t nd = (size_t)(3 * nn), ndc = (size_t)(3 * nnc);
   auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
   return al(81 * nd * sizeof(TS)) + 6 * al(nd * sizeof(T)) + 2 * al(ndc * sizeof(T)) + al((size_t)nn) +
-         al((size_t)nnc);
+         al((size_t)nnc) + (inv_smem ? al(ndc * ndc * sizeof(T)) : 0);
+}
+
+// 16-byte asynchronous copies global -> shared of the first (bytes / 16) * 16
+// bytes (both addresses 16-byte aligned), the tail by plain byte copies; the
+// caller waits with deep_copy_wait().
+__device__ __forceinline__ void deep_copy_async(void* dst, const void* src, size_t bytes) {
+  const size_t n16 = bytes / 16;
+  const unsigned char* s8 = reinterpret_cast<const unsigned char*>(src);
+  unsigned char* d8 = reinterpret_cast<unsigned char*>(dst);
+  for (size_t k = threadIdx.x; k < n16; k += blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(d8 + 16 * k);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(s8 + 16 * k) : "memory");
+  }
+  for (size_t k = n16 * 16 + threadIdx.x; k < bytes; k += blockDim.x) d8[k] = s8[k];
+}
+__device__ __forceinline__ void deep_copy_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// K u at DOF i from shared memory, in three partial sums (neighbours in the
+// planes z - 1, z, z + 1).
+template <typename T, typename TS>
+__device__ __forceinline__ T deep_row(const Grid& g, const TS* S, const T* u, int i) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const int NXY = NX * NY;
+  const int ndof = 3 * NXY * NZ;
+  const int n = i / 3;
+  const int iy = n % NY, r = n / NY;
+  const int ix = r % NX, iz = r / NX;
+  const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
+  const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
+  const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
+  T kv[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int oz = a == 0 ? oz0 : (a == 1 ? 0 : oz2);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const int ox = b == 0 ? ox0 : (b == 1 ? 0 : ox2);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int oy = e == 0 ? oy0 : (e == 1 ? 0 : oy2);
+        const int m3 = 3 * (n + oz + ox + oy);
+        const TS* s = S + (size_t)((a * 9 + b * 3 + e) * 3) * ndof + i;
+        kv[a] = fma(ld_coef<T, LdPlain>(s), u[m3], kv[a]);
+        kv[a] = fma(ld_coef<T, LdPlain>(s + ndof), u[m3 + 1], kv[a]);
+        kv[a] = fma(ld_coef<T, LdPlain>(s + 2 * (size_t)ndof), u[m3 + 2], kv[a]);
+      }
+    }
+  }
+  return (kv[0] + kv[1]) + kv[2];
 }
 
 template <typename T, typename TS>
@@ -82,19 +136,14 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   uint8_t* fix = q;
   q += al((size_t)nn);
   uint8_t* fixc = q;
+  q += al((size_t)nnc);
+  T* inv = p.inv_smem ? reinterpret_cast<T*>(q) : nullptr;
 
   const int t = threadIdx.x;
-  // stage the operator (16-byte copies) and the level's state
-  {
-    const size_t nbytes = 81 * (size_t)nd * sizeof(TS);  // a multiple of 2 * 81 * 3 bytes
-    const size_t n16 = nbytes / 16;
-    const uint4* src = reinterpret_cast<const uint4*>(p.S);
-    uint4* dst = reinterpret_cast<uint4*>(S);
-    for (size_t k = t; k < n16; k += kDeepThreads) dst[k] = __ldg(src + k);
-    const unsigned char* s8 = reinterpret_cast<const unsigned char*>(p.S);
-    unsigned char* d8 = reinterpret_cast<unsigned char*>(S);
-    for (size_t k = n16 * 16 + t; k < nbytes; k += kDeepThreads) d8[k] = s8[k];
-  }
+  // stage the operator and the coarsest inverse (asynchronous copies, all in
+  // flight while the level's state is loaded), then the level's state
+  deep_copy_async(S, p.S, 81 * (size_t)nd * sizeof(TS));
+  if (inv) deep_copy_async(inv, p.inv, (size_t)p.cn * p.cn * sizeof(T));
   for (int i = t; i < nd; i += kDeepThreads) {
     x[0][i] = p.x0[i];
     d[i] = p.d0 ? p.d0[i] : T(0);
@@ -103,6 +152,7 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   }
   for (int n = t; n < nn; n += kDeepThreads) fix[n] = p.fix[n];
   for (int n = t; n < nnc; n += kDeepThreads) fixc[n] = p.fixc[n];
+  deep_copy_wait();
   __syncthreads();
 
   int cur = 0;
@@ -119,7 +169,7 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
     double part = 0.0;
     for (int i = t; i < nd; i += kDeepThreads) {
       const int n = i / 3, c = i - 3 * n;
-      const T kv = stencil_row<T, TS, LdPlain>(p.g, S, x[cur], i);
+      const T kv = deep_row<T, TS>(p.g, S, x[cur], i);
       const bool fx = (fix[n] >> c) & 1;
       const T own = fx ? T(0) : x[cur][i];
       if (!p.cheb) op_epilogue<T, kModeJacobi>(io, i, fx, kv, own, epi_load<T, kModeJacobi>(io, i), part);
@@ -136,7 +186,7 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   for (int i = t; i < nd; i += kDeepThreads) {
     const int n = i / 3, c = i - 3 * n;
     const bool fx = (fix[n] >> c) & 1;
-    r[i] = fx ? T(0) : b[i] - stencil_row<T, TS, LdPlain>(p.g, S, x[cur], i);
+    r[i] = fx ? T(0) : b[i] - deep_row<T, TS>(p.g, S, x[cur], i);
   }
   __syncthreads();
   // restriction to the coarsest level
@@ -153,7 +203,8 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
     const int warp = t >> 5, lane = t & 31;
     for (int i = warp; i < p.cn; i += kDeepThreads / 32) {
       double acc = 0.0;
-      for (int j = lane; j < p.cn; j += 32) acc += (double)__ldg(&p.inv[(size_t)i * p.cn + j]) * (double)bc[j];
+      const T* row = (inv ? inv : p.inv) + (size_t)i * p.cn;
+      for (int j = lane; j < p.cn; j += 32) acc += (double)(inv ? row[j] : __ldg(&row[j])) * (double)bc[j];
       acc = warp_sum(acc);
       if (lane == 0) xc[i] = (T)acc;
     }

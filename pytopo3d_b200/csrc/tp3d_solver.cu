@@ -262,6 +262,7 @@ struct tp3d_solver {
   // 0 none), and that block's shared memory
   int deep_L = 0;
   size_t deep_smem = 0;
+  bool deep_inv_smem = false;
   int cyc_blocks64 = 0, cyc_blocks32 = 0;
   unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
@@ -678,6 +679,7 @@ struct tp3d_solver {
       p.coef = coef[L];
       p.inv = cinv32;
       p.cn = cn;
+      p.inv_smem = deep_inv_smem ? 1 : 0;
       p.b = b;
       p.x0 = lv.x[0];
       p.d0 = o.smoother != 1 ? lv.d : nullptr;
@@ -1554,10 +1556,14 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     const int L = s->nlev - 2;
     const bool b16 = s->S16[L] != nullptr;
     const long long nn = s->grids[L].nnode(), nnc = s->grids[L + 1].nnode();
-    const size_t smem = b16 ? deep_smem_bytes<float, __nv_bfloat16>(nn, nnc) : deep_smem_bytes<float, float>(nn, nnc);
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    auto bytes = [&](bool inv) {
+      return b16 ? deep_smem_bytes<float, __nv_bfloat16>(nn, nnc, inv) : deep_smem_bytes<float, float>(nn, nnc, inv);
+    };
+    s->deep_inv_smem = bytes(true) <= (size_t)optin;  // the coarsest inverse too, when it fits
+    const size_t smem = bytes(s->deep_inv_smem);
     const cudaError_t e = b16 ? cudaFuncSetAttribute(deep_cycle_kernel<float, __nv_bfloat16>,
                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
                               : cudaFuncSetAttribute(deep_cycle_kernel<float, float>,
