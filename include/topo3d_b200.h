@@ -191,6 +191,8 @@ typedef struct tp3d_solver_opts {
   int deep_cta;         /* mixed form, 1 (default): the last smoothed level and the coarsest solve run
                            as one thread block with the level's operator in shared memory (when it
                            fits), instead of one launch per smoothing step and grid transfer */
+  int block_sweeps;     /* smoother degree on the level run as one block (deep_cta); 0: as the
+                           other levels >= 2 (deep_sweeps) */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

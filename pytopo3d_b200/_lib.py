@@ -57,6 +57,7 @@ class SolverOpts(C.Structure):
         ("coarse_bf16", i32),
         ("split_dofs", i32),
         ("deep_cta", i32),
+        ("block_sweeps", i32),
     ]
 
 

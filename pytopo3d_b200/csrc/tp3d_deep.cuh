@@ -12,8 +12,10 @@
 // multiplies by the coarsest inverse, prolongs and smooths again, and writes
 // the level's iterate back.  Every phase calls the same per-node device
 // functions and epilogues as the separate kernels, with plain loads from
-// shared memory; a stencil row is summed in three partial sums (one per
-// z-plane of neighbours) to shorten its dependent chain, so rows round
+// shared memory.  With a bf16 stencil the block reads it node-major (one
+// thread per node computes the node's three rows from 31 16-byte loads and
+// 81 neighbour values, kDeepRow entries per node); rows are summed in partial
+// sums (FP32: one per z-plane of neighbours; bf16: two per row), so they round
 // differently from the separate kernels' single sum.
 #pragma once
 
@@ -22,11 +24,72 @@
 namespace tp3d {
 
 constexpr int kDeepThreads = 1024;
+constexpr int kDeepRow = 248;  // node-major bf16 stencil: 243 entries (k = (jrel * 3 + c) * 3 + d) + 5 zeros
+
+// The node-major bf16 stencil of a level from its FP64 stencil (fixed rows and
+// columns and neighbours past the grid zeroed, as in the packed layout).
+__global__ void deep_pack_kernel(Grid g, const double* __restrict__ A, const uint8_t* __restrict__ fix,
+                                 __nv_bfloat16* SN) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const long long nn = g.nnode();
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < nn * kDeepRow;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long n = idx / kDeepRow;
+    const int k = (int)(idx - n * kDeepRow);
+    double v = 0.0;
+    if (k < 243) {
+      const int jr = k / 9, c = (k / 3) % 3, d = k % 3;
+      const int dz = jr / 9 - 1, dx = (jr / 3) % 3 - 1, dy = jr % 3 - 1;
+      const int iy = (int)(n % NY);
+      const long long r = n / NY;
+      const int ix = (int)(r % NX), iz = (int)(r / NX);
+      const int x = ix + dx, y = iy + dy, z = iz + dz;
+      const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
+      const int fm = in ? fix[g.nidx(x, y, z)] : 7;
+      if (!((fix[n] >> c) & 1) && !((fm >> d) & 1)) v = A[(long long)k * nn + n];
+    }
+    SN[idx] = __double2bfloat16(v);
+  }
+}
+
+// K u at the three DOFs of node n from the node-major bf16 stencil in shared
+// memory, two partial sums per row.
+template <typename T>
+__device__ __forceinline__ void deep_node_rows(const Grid& g, const __nv_bfloat16* SN, const T* u, int n, T y[3]) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const int NXY = NX * NY;
+  const int iy = n % NY, r = n / NY;
+  const int ix = r % NX, iz = r / NX;
+  const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
+  const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
+  const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
+  const uint4* row = reinterpret_cast<const uint4*>(SN + (size_t)n * kDeepRow);
+  T acc[3][2] = {{T(0), T(0)}, {T(0), T(0)}, {T(0), T(0)}};
+#pragma unroll
+  for (int q = 0; q < kDeepRow / 8; ++q) {
+    const uint4 w = row[q];
+    const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+      const int k = 8 * q + h;
+      if (k < 243) {
+        const int jr = k / 9, c = (k / 3) % 3, d = k % 3;
+        const int a = jr / 9, bb = (jr / 3) % 3, e = jr % 3;
+        const int m = n + (a == 0 ? oz0 : (a == 1 ? 0 : oz2)) + (bb == 0 ? ox0 : (bb == 1 ? 0 : ox2)) +
+                      (e == 0 ? oy0 : (e == 1 ? 0 : oy2));
+        const unsigned bits = (h & 1) ? (ws[h >> 1] & 0xffff0000u) : (ws[h >> 1] << 16);
+        acc[c][jr & 1] = fma((T)__uint_as_float(bits), u[3 * m + d], acc[c][jr & 1]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) y[c] = acc[c][0] + acc[c][1];
+}
 
 template <typename T, typename TS>
 struct DeepParams {
   Grid g{}, gc{};               // the level and the coarsest level
-  const TS* S = nullptr;        // the level's packed stencil
+  const TS* S = nullptr;        // the level's stencil: bf16 node-major (kDeepRow per node) or FP32 packed
   const uint8_t* fix = nullptr;   // the level's node masks
   const uint8_t* fixc = nullptr;  // the coarsest level's node masks
   const T* dinv = nullptr;
@@ -44,15 +107,22 @@ struct DeepParams {
   const int* done = nullptr;
 };
 
+// Bytes of the level's stencil in the block: node-major bf16 (kDeepRow per
+// node) or DOF-major packed (81 per DOF).
+template <typename TS>
+__host__ __device__ constexpr size_t deep_stencil_bytes(long long nn) {
+  return sizeof(TS) == 2 ? (size_t)nn * kDeepRow * 2 : (size_t)(81 * 3 * nn) * sizeof(TS);
+}
+
 // Shared-memory bytes of the block for a level of `nn` nodes and a coarsest
-// level of `nnc` nodes: stencil (81 coefficients per DOF), six level vectors
-// (x[2], b, d, dinv, r), two coarsest vectors, node masks, and with inv_smem
-// the coarsest inverse; 16-byte aligned parts.
+// level of `nnc` nodes: stencil, six level vectors (x[2], b, d, dinv, r), two
+// coarsest vectors, node masks, and with inv_smem the coarsest inverse;
+// 16-byte aligned parts.
 template <typename T, typename TS>
 __host__ __device__ constexpr size_t deep_smem_bytes(long long nn, long long nnc, bool inv_smem) {
   const size_t nd = (size_t)(3 * nn), ndc = (size_t)(3 * nnc);
   auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
-  return al(81 * nd * sizeof(TS)) + 6 * al(nd * sizeof(T)) + 2 * al(ndc * sizeof(T)) + al((size_t)nn) +
+  return al(deep_stencil_bytes<TS>(nn)) + 6 * al(nd * sizeof(T)) + 2 * al(ndc * sizeof(T)) + al((size_t)nn) +
          al((size_t)nnc) + (inv_smem ? al(ndc * ndc * sizeof(T)) : 0);
 }
 
@@ -114,8 +184,9 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   const int nd = (int)(3 * nn), ndc = (int)(3 * nnc);
   auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
   unsigned char* q = smem;
+  constexpr bool kNode = sizeof(TS) == 2;  // bf16: node-major
   TS* S = reinterpret_cast<TS*>(q);
-  q += al(81 * (size_t)nd * sizeof(TS));
+  q += al(deep_stencil_bytes<TS>(nn));
   T* x[2];
   x[0] = reinterpret_cast<T*>(q);
   q += al(nd * sizeof(T));
@@ -142,7 +213,7 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   const int t = threadIdx.x;
   // stage the operator and the coarsest inverse (asynchronous copies, all in
   // flight while the level's state is loaded), then the level's state
-  deep_copy_async(S, p.S, 81 * (size_t)nd * sizeof(TS));
+  deep_copy_async(S, p.S, deep_stencil_bytes<TS>(nn));
   if (inv) deep_copy_async(inv, p.inv, (size_t)p.cn * p.cn * sizeof(T));
   for (int i = t; i < nd; i += kDeepThreads) {
     x[0][i] = p.x0[i];
@@ -167,14 +238,25 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
     io.step = s;
     io.omega = p.omega;
     double part = 0.0;
-    for (int i = t; i < nd; i += kDeepThreads) {
-      const int n = i / 3, c = i - 3 * n;
-      const T kv = deep_row<T, TS>(p.g, S, x[cur], i);
+    auto epi = [&](int i, int n, int c, T kv) {
       const bool fx = (fix[n] >> c) & 1;
       const T own = fx ? T(0) : x[cur][i];
       if (!p.cheb) op_epilogue<T, kModeJacobi>(io, i, fx, kv, own, epi_load<T, kModeJacobi>(io, i), part);
       else if (first) op_epilogue<T, kModeChebFirst>(io, i, fx, kv, own, epi_load<T, kModeChebFirst>(io, i), part);
       else op_epilogue<T, kModeChebStep>(io, i, fx, kv, own, epi_load<T, kModeChebStep>(io, i), part);
+    };
+    if constexpr (kNode) {
+      for (int n = t; n < nn; n += kDeepThreads) {
+        T y[3];
+        deep_node_rows<T>(p.g, reinterpret_cast<const __nv_bfloat16*>(S), x[cur], n, y);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) epi(3 * n + c, n, c, y[c]);
+      }
+    } else {
+      for (int i = t; i < nd; i += kDeepThreads) {
+        const int n = i / 3, c = i - 3 * n;
+        epi(i, n, c, deep_row<T, TS>(p.g, S, x[cur], i));
+      }
     }
     __syncthreads();
     cur ^= 1;
@@ -183,10 +265,19 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   // pre-smoothing (step 0 was taken by the restriction)
   for (int s = 1; s < p.pre; ++s) smooth(s, false);
   // residual
-  for (int i = t; i < nd; i += kDeepThreads) {
-    const int n = i / 3, c = i - 3 * n;
-    const bool fx = (fix[n] >> c) & 1;
-    r[i] = fx ? T(0) : b[i] - deep_row<T, TS>(p.g, S, x[cur], i);
+  if constexpr (kNode) {
+    for (int n = t; n < nn; n += kDeepThreads) {
+      T y[3];
+      deep_node_rows<T>(p.g, reinterpret_cast<const __nv_bfloat16*>(S), x[cur], n, y);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[3 * n + c] = ((fix[n] >> c) & 1) ? T(0) : b[3 * n + c] - y[c];
+    }
+  } else {
+    for (int i = t; i < nd; i += kDeepThreads) {
+      const int n = i / 3, c = i - 3 * n;
+      const bool fx = (fix[n] >> c) & 1;
+      r[i] = fx ? T(0) : b[i] - deep_row<T, TS>(p.g, S, x[cur], i);
+    }
   }
   __syncthreads();
   // restriction to the coarsest level

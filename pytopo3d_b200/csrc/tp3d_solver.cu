@@ -263,6 +263,7 @@ struct tp3d_solver {
   int deep_L = 0;
   size_t deep_smem = 0;
   bool deep_inv_smem = false;
+  __nv_bfloat16* deep_SN = nullptr;  // its node-major bf16 stencil (bf16 levels)
   int cyc_blocks64 = 0, cyc_blocks32 = 0;
   unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
@@ -657,10 +658,12 @@ struct tp3d_solver {
 
   // smoothing degrees of level L (coarse_sweeps > 0 overrides both on levels >= 1)
   int pre_sweeps(int L) const {
+    if (L == deep_L && deep_L > 0 && o.block_sweeps > 0) return o.block_sweeps;
     if (L > 1 && o.deep_sweeps > 0) return o.deep_sweeps;
     return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.pre_sweeps;
   }
   int post_sweeps(int L) const {
+    if (L == deep_L && deep_L > 0 && o.block_sweeps > 0) return o.block_sweeps;
     if (L > 1 && o.deep_sweeps > 0) return o.deep_sweeps;
     return (L > 0 && o.coarse_sweeps > 0) ? o.coarse_sweeps : o.post_sweeps;
   }
@@ -693,7 +696,7 @@ struct tp3d_solver {
     if (S16[L]) {
       DeepParams<float, __nv_bfloat16> p;
       fill(p);
-      p.S = S16[L];
+      p.S = deep_SN;
       launch(kPdlCoarse, deep_cycle_kernel<float, __nv_bfloat16>, dim3(1), dim3(kDeepThreads), deep_smem, p);
     } else {
       DeepParams<float, float> p;
@@ -1344,6 +1347,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->coarse_bf16 = 99;
   o->split_dofs = 16384;
   o->deep_cta = 1;
+  o->block_sweeps = 0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1366,6 +1370,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     return fail(TP3D_ERR_ARG, "invalid solver options");
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
+  if (o.block_sweeps < 0 || o.block_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid block_sweeps");
   if (o.pdl < 0 || o.pdl > 3) return fail(TP3D_ERR_ARG, "invalid pdl");
   if (o.split_dofs < 0) return fail(TP3D_ERR_ARG, "invalid split_dofs");
   if (o.coarse_bf16 < 0) return fail(TP3D_ERR_ARG, "invalid coarse_bf16");
@@ -1569,8 +1574,11 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
                               : cudaFuncSetAttribute(deep_cycle_kernel<float, float>,
                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (smem <= (size_t)optin && e == cudaSuccess) {
-      s->deep_L = L;
-      s->deep_smem = smem;
+      if (b16) s->deep_SN = s->alloc<__nv_bfloat16>((size_t)nn * kDeepRow);
+      if (!b16 || s->deep_SN) {
+        s->deep_L = L;
+        s->deep_smem = smem;
+      }
     }
     cudaGetLastError();
   }
@@ -1784,6 +1792,10 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       if (s->L64[L].A) s->pack_level<double>(L, s->L64[L].A);  // the mixed form's FP64 fallback
     } else if (!packed) {
       s->pack_level<double>(L, s->L64[L].A);
+    }
+    if (L == s->deep_L && s->deep_SN) {
+      deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->deep_SN);
+      count_launch();
     }
     TP3D_CHECK_LAUNCH();
     if (int rc = fork_spectra(s, L)) return rc;
