@@ -218,6 +218,19 @@ int tp3d_solver_solve(tp3d_solver* s, const double* F, double* U, int* iteration
                       double* relres);
 
 /* y = K u with fixed rows/cols replaced by identity (FP64 / FP32 forms). */
+/* tp3d_solver_solve in two halves, so that a caller can queue work that reads U
+ * (sensitivities) before the host waits for the solve.  _begin queues the solve
+ * (the mixed form: its FP32 iteration and FP64 result; the FP64 form solves
+ * completely here) and returns at once; U holds the result in stream order.
+ * _end waits, reads the iteration count and residual, and returns the status
+ * tp3d_solver_solve would have returned.  When the mixed form had to finish
+ * the system with the FP64 solver, that solve runs in _end after the work the
+ * caller queued since _begin, overwrites U and sets *replaced = 1: the caller
+ * then repeats its work that read U.  No other solver call may come between
+ * the two halves. */
+int tp3d_solver_solve_begin(tp3d_solver* s, const double* F, double* U);
+int tp3d_solver_solve_end(tp3d_solver* s, int* iterations, double* relres, int* replaced);
+
 int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
 int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
 

@@ -84,6 +84,8 @@ SIGNATURES = {
     "tp3d_solver_destroy": (i32, [vp]),
     "tp3d_solver_set_density": (i32, [vp, vp, f64]),
     "tp3d_solver_solve": (i32, [vp, vp, vp, C.POINTER(i32), C.POINTER(f64)]),
+    "tp3d_solver_solve_begin": (i32, [vp, vp, vp]),
+    "tp3d_solver_solve_end": (i32, [vp, C.POINTER(i32), C.POINTER(f64), C.POINTER(i32)]),
     "tp3d_solver_apply_f64": (i32, [vp, vp, vp]),
     "tp3d_solver_apply_f32": (i32, [vp, vp, vp]),
     "tp3d_solver_time_apply": (i32, [vp, i32, i32, C.POINTER(f64)]),

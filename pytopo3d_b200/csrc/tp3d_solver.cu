@@ -1175,7 +1175,8 @@ struct tp3d_solver {
     return rc;
   }
 
-  int solve_mixed(const double* F) {
+  // The mixed solve up to its result in u64, without waiting for it.
+  int solve_mixed_launch(const double* F) {
     const long long nn = g.nnode(), ndof = 3 * nn;
     const int nb = grid_blocks(ndof);
     last_floor = false;
@@ -1210,6 +1211,18 @@ struct tp3d_solver {
     rc = replay<float>(K32, o.max_iterations);
     if (rc) return rc;
     flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K32.u, state, 1); count_launch();
+    TP3D_CHECK_LAUNCH();
+    return TP3D_OK;
+  }
+
+  // The mixed solve launched by solve_mixed_launch: reads its state (host
+  // synchronisation) and, if FP32 could not resolve the system, finishes it
+  // with the FP64 solver (*fallback set).  `before_fallback` runs first then
+  // (the split entry point joins the caller's stream there).
+  template <class Before>
+  int solve_mixed_finish(const double* F, bool* fallback, Before before_fallback) {
+    const long long ndof = 3 * g.nnode();
+    *fallback = false;
     TP3D_CHECK(cudaStreamSynchronize(st));
     const PcgState s = state_host[0];
     last_iters = s.iters;
@@ -1219,14 +1232,28 @@ struct tp3d_solver {
     if (s.done == 1 || s.done == 5 || s.done == 7) return status_of(s);
     // FP32 could not resolve this system (cap, breakdown, non-finite, or a
     // stall far above the target): finish it with the FP64 solver.
+    *fallback = true;
+    if (int e = before_fallback()) return e;
     if (int e = ensure_fp64_buffers()) return e;
     if (s.done == 3 || s.done == 4) TP3D_CHECK(cudaMemsetAsync(u64, 0, ndof * sizeof(double), st));
     const int mixed_iters = s.iters;
     last_fallback = true;
-    rc = solve64(F);
+    const int rc = solve64(F);
     last_iters += mixed_iters;
     return rc;
   }
+
+  int solve_mixed(const double* F) {
+    if (int rc = solve_mixed_launch(F)) return rc;
+    bool fb = false;
+    return solve_mixed_finish(F, &fb, [] { return TP3D_OK; });
+  }
+
+  // split solve (tp3d_solver_solve_begin / _end)
+  bool pending = false;
+  const double* pend_F = nullptr;
+  double* pend_U = nullptr;
+  int pend_rc = TP3D_OK;
 
   // FP64 Krylov and level vectors for the mixed form's fallback (allocated on first use).
   int ensure_fp64_buffers() {
@@ -1834,6 +1861,63 @@ extern "C" int tp3d_solver_solve(tp3d_solver* s, const double* F, double* U, int
   TP3D_CHECK(cudaMemcpyAsync(U, s->u64, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
   TP3D_CHECK(cudaStreamSynchronize(st));
   if (int e = s->leave()) return e;
+  if (iterations) *iterations = s->last_iters;
+  if (relres) *relres = s->last_relres;
+  return rc;
+}
+
+extern "C" int tp3d_solver_solve_begin(tp3d_solver* s, const double* F, double* U) {
+  if (!s || !F || !U) return TP3D_ERR_ARG;
+  if (!s->have_density) {
+    tp3d_set_last_error("tp3d_solver_set_density must be called before solve");
+    return TP3D_ERR_ARG;
+  }
+  if (s->pending) {
+    tp3d_set_last_error("tp3d_solver_solve_end must follow tp3d_solver_solve_begin");
+    return TP3D_ERR_ARG;
+  }
+  if (!s->mixed) {  // the FP64 form reads its residual between restarts: it completes here
+    s->pend_rc = tp3d_solver_solve(s, F, U, nullptr, nullptr);
+    return s->pend_rc < 0 ? s->pend_rc : TP3D_OK;
+  }
+  cudaStream_t st = s->st;
+  const long long nn = s->g.nnode(), ndof = 3 * nn;
+  if (int e = s->enter()) return e;
+  if (s->cyc_bar) TP3D_CHECK(cudaMemsetAsync(s->cyc_bar, 0, 2 * sizeof(unsigned int), st));
+  TP3D_CHECK(cudaMemcpyAsync(s->u64, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  zero_fixed_kernel<<<s->grid_blocks(nn), 256, 0, st>>>(nn, s->u64, s->fix[0]); count_launch();
+  s->last_updates = 0;
+  s->last_restarts = 0;
+  if (int rc = s->solve_mixed_launch(F)) return rc;
+  TP3D_CHECK(cudaMemcpyAsync(U, s->u64, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (int e = s->leave()) return e;
+  s->pending = true;
+  s->pend_F = F;
+  s->pend_U = U;
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_solver_solve_end(tp3d_solver* s, int* iterations, double* relres, int* replaced) {
+  if (!s) return TP3D_ERR_ARG;
+  if (replaced) *replaced = 0;
+  int rc = s->pend_rc;
+  if (s->pending) {
+    s->pending = false;
+    cudaStream_t st = s->st;
+    const long long ndof = 3 * s->g.nnode();
+    bool fb = false;
+    // a fallback solve waits for the caller's work queued since begin (it read U)
+    rc = s->solve_mixed_finish(s->pend_F, &fb, [&] { return s->enter(); });
+    if (fb) {
+      if (rc >= 0 || rc == TP3D_ERR_NONFINITE)
+        TP3D_CHECK(cudaMemcpyAsync(s->pend_U, s->u64, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      TP3D_CHECK(cudaStreamSynchronize(st));
+      if (int e = s->leave()) return e;
+      if (replaced) *replaced = 1;
+    }
+    if (rc < 0 && rc != TP3D_ERR_NONFINITE) return rc;
+  }
+  s->pend_rc = TP3D_OK;
   if (iterations) *iterations = s->last_iters;
   if (relres) *relres = s->last_relres;
   return rc;

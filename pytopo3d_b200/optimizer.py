@@ -107,15 +107,23 @@ class SimpState:
         for k in range(self.F.shape[0]):
             _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
                                          1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
-            self.solver.solve(self.F[k], self.U[k])
-            iters += self.solver.last_iterations
             dst_dc = self.dc_dx if k == 0 else self.dc_acc
-            _lib.check(L.tp3d_sensitivity(
-                H.nelx, H.nely, H.nelz, H.rmin, self.U[k].data_ptr(), self.KE.ctypes.data,
-                rho_p.data_ptr(), dproj.data_ptr(), self.Hs.data_ptr(), self.free.data_ptr(), self.penal,
-                self.ce.data_ptr(), dst_dc.data_ptr(), self.dv_dx.data_ptr(),
-                self.c_dev[min(k, 1)].data_ptr(), self.sens_scratch.data_ptr(), _lib.stream_ptr()),
-                "sensitivity")
+
+            def sens():
+                _lib.check(L.tp3d_sensitivity(
+                    H.nelx, H.nely, H.nelz, H.rmin, self.U[k].data_ptr(), self.KE.ctypes.data,
+                    rho_p.data_ptr(), dproj.data_ptr(), self.Hs.data_ptr(), self.free.data_ptr(), self.penal,
+                    self.ce.data_ptr(), dst_dc.data_ptr(), self.dv_dx.data_ptr(),
+                    self.c_dev[min(k, 1)].data_ptr(), self.sens_scratch.data_ptr(), _lib.stream_ptr()),
+                    "sensitivity")
+
+            # the sensitivities are queued behind the solve before the host waits
+            # for it; a mixed solve finished in FP64 replaces U, and they are redone
+            self.solver.solve_begin(self.F[k], self.U[k])
+            sens()
+            if self.solver.solve_end():
+                sens()
+            iters += self.solver.last_iterations
             if k > 0:
                 self.dc_dx += self.dc_acc
                 self.c_dev[0] += self.c_dev[1]

@@ -109,6 +109,26 @@ class HexSolver:
             raise RuntimeError(f"CG failed to converge: iterations={it.value}, relres={rr.value:.3e}")
         return U
 
+    def solve_begin(self, F: torch.Tensor, U: torch.Tensor):
+        """Queue the solve of K U = F (U: warm start, updated in place in stream
+        order) without waiting for it; ``solve_end`` completes it."""
+        self._pending_F = vec(F)
+        _lib.check(_lib.lib().tp3d_solver_solve_begin(self._h, self._pending_F.data_ptr(), U.data_ptr()),
+                   "solve")
+
+    def solve_end(self, raise_on_fail: bool = True) -> bool:
+        """Wait for the queued solve; True when the mixed form finished it with
+        the FP64 solver after the work queued since ``solve_begin`` (which then
+        read a U that has since been replaced)."""
+        it, rr, rep = C.c_int(0), C.c_double(0), C.c_int(0)
+        rc = _lib.check(_lib.lib().tp3d_solver_solve_end(self._h, C.byref(it), C.byref(rr), C.byref(rep)),
+                        "solve")
+        self._pending_F = None
+        self.last_iterations, self.last_relres = it.value, rr.value
+        if rc == _lib.TP3D_NOT_CONVERGED and raise_on_fail:
+            raise RuntimeError(f"CG failed to converge: iterations={it.value}, relres={rr.value:.3e}")
+        return bool(rep.value)
+
     def apply(self, u: torch.Tensor) -> torch.Tensor:
         y = torch.empty_like(u)
         fn = _lib.lib().tp3d_solver_apply_f64 if u.dtype == torch.float64 else _lib.lib().tp3d_solver_apply_f32

@@ -241,6 +241,42 @@ def test_deep_block_cycle_matches_per_phase_launches(P, dims, fits, smoother):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
 
 
+# The split solve (queue, let the caller queue work on U, then wait) gives the
+# blocking solve's result; when the mixed form has to finish in FP64 (here: an
+# iteration cap it cannot meet) the FP64 solve runs after the caller's queued
+# work and reports that U was replaced.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("cap", [5000, 4])
+def test_split_solve_matches_blocking_solve(P, prec, cap):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 24, 12, 12
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=10, lo=0.0)
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    out = []
+    for split in (False, True):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, max_iterations=cap, fine_operator=3)
+        s.set_density(to_flat(rho), 3.0)
+        U = torch.zeros_like(F)
+        seen = None
+        if split:
+            s.solve_begin(F, U)
+            seen = torch.dot(U, F)  # queued behind the solve
+            replaced = s.solve_end(raise_on_fail=False)
+            assert replaced == (prec == "mixed" and cap == 4)
+        else:
+            s.solve(F, U, raise_on_fail=False)
+        out.append((U.cpu().numpy(), s.last_iterations, seen))
+        s.close()
+    (U0, it0, _), (U1, it1, seen) = out
+    assert it0 == it1
+    np.testing.assert_array_equal(U1, U0)
+    if not (prec == "mixed" and cap == 4):
+        assert float(seen) == float(np.dot(U0, F.cpu().numpy())) or abs(float(seen) - float(np.dot(U0, F.cpu().numpy()))) <= 1e-12 * abs(float(seen))
+
+
 # Programmatic dependent launch only changes when a kernel may be scheduled,
 # never what it computes or in which order the kernels' writes land: every
 # mask gives bit-identical iterations and solutions, with the device loop.
