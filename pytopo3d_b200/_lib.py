@@ -58,6 +58,7 @@ class SolverOpts(C.Structure):
         ("split_dofs", i32),
         ("deep_cta", i32),
         ("block_sweeps", i32),
+        ("resid_restrict_dofs", i32),
     ]
 
 

@@ -530,6 +530,62 @@ __global__ void __launch_bounds__(256) restrict_kernel(Grid gf, Grid gc, const T
   }
 }
 
+// Residual and restriction in one launch, for small levels: one block per
+// coarse node, thread q < 81 of it computes the residual of fine DOF q of the
+// node's 3 x 3 x 3 fine neighbourhood (node q / 3 in the (z, x, y) order of
+// restrict_node, component q % 3) from the fine stencil, weighted by the
+// trilinear restriction weight; the block sums the 27 weighted residuals of
+// each component in a fixed order.  Each fine residual is computed by up to 8
+// coarse nodes' blocks: on a level of a few thousand DOFs that costs less than
+// the launch it saves.  The coarse level's first smoothing step rides along as
+// in restrict_kernel.
+constexpr int kRestrictResidThreads = 96;
+
+template <typename T, typename TS>
+__global__ void __launch_bounds__(kRestrictResidThreads) restrict_resid_kernel(
+    const __grid_constant__ StencilParams<T, TS> p, Grid gc, const uint8_t* __restrict__ fixc, T* bc,
+    CoarseFirstStep<T> fs) {
+  pdl_entry();
+  if (op_skip(p.io)) return;
+  __shared__ T part[81];
+  const Grid& gf = p.g;
+  const int FX = gf.nx + 1, FY = gf.ny + 1, FZ = gf.nz + 1;
+  const int CX = gc.nx + 1, CY = gc.ny + 1;
+  const int N = blockIdx.x;
+  const int Iy = N % CY, rN = N / CY;
+  const int Ix = rN % CX, Iz = rN / CX;
+  const int q = threadIdx.x;
+  if (q < 81) {
+    const int j = q / 3, c = q - 3 * j;
+    const int dz = j / 9 - 1, dx = (j / 3) % 3 - 1, dy = j % 3 - 1;
+    const int x = 2 * Ix + dx, y = 2 * Iy + dy, z = 2 * Iz + dz;
+    T v = T(0);
+    if (x >= 0 && x < FX && y >= 0 && y < FY && z >= 0 && z < FZ) {
+      const int n = y + FY * (x + FX * z);
+      const int i = 3 * n + c;
+      if (!((p.fix[n] >> c) & 1)) {
+        const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+        v = w * (p.io.b[i] - stencil_row<T, TS>(gf, p.S, p.io.u, i));
+      }
+    }
+    part[q] = v;
+  }
+  __syncthreads();
+  if (q < 3) {
+    T sum = T(0);
+    for (int j = 0; j < 27; ++j) sum += part[3 * j + q];
+    const int i = 3 * N + q;
+    const T bv = ((fixc[N] >> q) & 1) ? T(0) : sum;
+    bc[i] = bv;
+    if (fs.x0) {
+      const T w = fs.coef ? (T)fs.coef[0] : fs.omega;
+      const T v0 = w * fs.dinv[i] * bv;
+      fs.x0[i] = v0;
+      if (fs.d) fs.d[i] = v0;
+    }
+  }
+}
+
 // x_f[i] += sum_I P[i,I] x_c[I] on free fine DOFs.  A fine node takes 1, 2, 4
 // or 8 coarse nodes (weights 1 or 1/2 per axis), read as a fixed 2x2x2 block
 // with zero weights for the absent ones.  Grid: plane_grid(FX*FY, FZ).

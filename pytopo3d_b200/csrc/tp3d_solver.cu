@@ -745,7 +745,11 @@ struct tp3d_solver {
              cheb ? lv.d : (T*)nullptr, done);
     }
     *rc |= smooth_steps<T>(L, 1, pre_sweeps(L) - 1, &cur, b, done);
-    {
+    auto& lc = levels<T>()[L + 1];
+    const Grid& gn = grids[L + 1];
+    // small coarse levels: residual and restriction in one launch
+    const bool resid_fused = L > 0 && ndof <= o.resid_restrict_dofs;
+    if (!resid_fused) {
       OpIO<T> io;
       io.u = lv.x[cur];
       io.out = lv.r;
@@ -753,8 +757,6 @@ struct tp3d_solver {
       io.done = done;
       *rc |= apply_level<T, kModeResid>(L, io);
     }
-    auto& lc = levels<T>()[L + 1];
-    const Grid& gn = grids[L + 1];
     // the next level's first smoothing step rides along when that level smooths
     const bool fuse_first = L + 1 < nlev - 1 && !(L + 1 == cyc_L0 && cyc_L0 > 0);
     CoarseFirstStep<T> fs;
@@ -765,8 +767,37 @@ struct tp3d_solver {
       fs.x0 = lc.x[0];
       fs.d = cheb ? lc.d : nullptr;
     }
-    launch(kPdlCoarse, restrict_kernel<T>, plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), dim3(256), 0, gl, gn,
-           (const T*)lv.r, (const uint8_t*)fix[L + 1], lc.b, done, fs);
+    if (resid_fused) {
+      auto fill = [&](auto& p) {
+        p.g = gl;
+        p.fix = fix[L];
+        p.io.u = lv.x[cur];
+        p.io.b = b;
+        p.io.done = done;
+      };
+      const dim3 grid((unsigned)gn.nnode());
+      bool done16 = false;
+      if constexpr (sizeof(T) == 4) {
+        if (S16[L]) {
+          StencilParams<float, __nv_bfloat16> p;
+          fill(p);
+          p.S = S16[L];
+          launch(kPdlCoarse, restrict_resid_kernel<float, __nv_bfloat16>, grid, dim3(kRestrictResidThreads), 0, p,
+                 gn, (const uint8_t*)fix[L + 1], lc.b, fs);
+          done16 = true;
+        }
+      }
+      if (!done16) {
+        StencilParams<T> p;
+        fill(p);
+        p.S = lv.A;
+        launch(kPdlCoarse, restrict_resid_kernel<T, T>, grid, dim3(kRestrictResidThreads), 0, p, gn,
+               (const uint8_t*)fix[L + 1], lc.b, fs);
+      }
+    } else {
+      launch(kPdlCoarse, restrict_kernel<T>, plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), dim3(256), 0, gl,
+             gn, (const T*)lv.r, (const uint8_t*)fix[L + 1], lc.b, done, fs);
+    }
     T* xc = vcycle<T>(L + 1, lc.b, done, rc, fuse_first);
     launch(L == 0 ? kPdlFine : kPdlCoarse, prolong_add_kernel<T>, plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1),
            dim3(256), 0, gl, gn, (const T*)xc, (const uint8_t*)fix[L], lv.x[cur], done);
@@ -1375,6 +1406,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->split_dofs = 16384;
   o->deep_cta = 1;
   o->block_sweeps = 0;
+  o->resid_restrict_dofs = 0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1398,6 +1430,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
   if (o.block_sweeps < 0 || o.block_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid block_sweeps");
+  if (o.resid_restrict_dofs < 0) return fail(TP3D_ERR_ARG, "invalid resid_restrict_dofs");
   if (o.pdl < 0 || o.pdl > 3) return fail(TP3D_ERR_ARG, "invalid pdl");
   if (o.split_dofs < 0) return fail(TP3D_ERR_ARG, "invalid split_dofs");
   if (o.coarse_bf16 < 0) return fail(TP3D_ERR_ARG, "invalid coarse_bf16");

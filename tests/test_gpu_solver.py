@@ -241,6 +241,33 @@ def test_deep_block_cycle_matches_per_phase_launches(P, dims, fits, smoother):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
 
 
+# Residual and restriction in one launch on the small levels are the same
+# operations as the two launches, summed in another order: same iterations
+# (within one or 2%), same solution to rounding.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("dims", [(48, 24, 24), (33, 17, 9)])
+def test_fused_residual_restriction_matches_two_launches(P, dims, prec):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=12, lo=0.0)
+    rho[rho < 0.25] = 0.0
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    its, Us = [], []
+    for thr in (0, 1 << 30):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, resid_restrict_dofs=thr, fine_operator=3)
+        s.set_density(to_flat(rho), 3.0)
+        U = s.solve(F)
+        its.append(s.last_iterations)
+        Us.append(U.cpu().numpy())
+        s.close()
+    assert abs(its[0] - its[1]) <= max(1, 0.02 * its[0]), its
+    tol = 1e-9 if prec == "fp64" else 1e-5
+    np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=tol * np.abs(Us[0]).max())
+
+
 # The split solve (queue, let the caller queue work on U, then wait) gives the
 # blocking solve's result; when the mixed form has to finish in FP64 (here: an
 # iteration cap it cannot meet) the FP64 solve runs after the caller's queued
