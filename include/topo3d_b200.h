@@ -198,6 +198,8 @@ typedef struct tp3d_solver_opts {
                            computed by up to 8 coarse nodes).  Default 0 (off): at 128x64x64 the
                            two launches are faster (measured 0.4% per SIMP iteration mixed, 0.7%
                            FP64) */
+  int spectra_streams;  /* 1 (default): each level's power iteration at set-up on its own stream, as
+                           soon as the level is built; 0: all of them in order on the solver's stream */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

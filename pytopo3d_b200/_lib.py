@@ -59,6 +59,7 @@ class SolverOpts(C.Structure):
         ("deep_cta", i32),
         ("block_sweeps", i32),
         ("resid_restrict_dofs", i32),
+        ("spectra_streams", i32),
     ]
 
 

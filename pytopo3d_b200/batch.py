@@ -105,6 +105,9 @@ class BatchRunner:
                  move: float = 0.2, workers: int = 8, solver_options: Optional[dict] = None):
         self.specs = list(specs)
         self.workers = max(1, min(int(workers), len(self.specs)))
+        # the designs already run side by side: each solver's set-up keeps its
+        # power iterations on its own stream (fewer host calls per design)
+        solver_options = {"spectra_streams": 0, **(solver_options or {})}
         self.streams = [torch.cuda.Stream(device=device()) for _ in self.specs]
         self.loops: List[SimpLoop] = [None] * len(self.specs)
         self.ndof = [3 * (s.nelx + 1) * (s.nely + 1) * (s.nelz + 1) for s in self.specs]

@@ -1,6 +1,8 @@
 // Library-wide C ABI helpers: error reporting and version.
 #include <atomic>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "tp3d_common.cuh"
 
@@ -19,6 +21,28 @@ std::atomic<long long> g_launches{0};
 }
 namespace tp3d {
 void add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int ensure_dynamic_smem(const void* func, int bytes) {
+  static std::mutex m;
+  static std::unordered_map<const void*, int> limit;
+  std::lock_guard<std::mutex> g(m);
+  auto it = limit.find(func);
+  if (it != limit.end() && it->second >= bytes) return TP3D_OK;
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa{};
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, func) != cudaSuccess)
+    return TP3D_ERR_CUDA;
+  const int most = optin - (int)fa.sharedSizeBytes;  // the kernel's static shared memory counts too
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+  if (e != cudaSuccess) {
+    tp3d_set_last_error(cudaGetErrorString(e));
+    return TP3D_ERR_CUDA;
+  }
+  limit[func] = most;
+  return bytes <= most ? TP3D_OK : TP3D_ERR_ARG;
+}
 }  // namespace tp3d
 
 extern "C" long long tp3d_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }

@@ -220,6 +220,17 @@ inline cudaError_t launch_kernel_c(bool pdl, const void* kern, dim3 grid, dim3 b
 // replays add the graph's kernel-node count).
 void add_launches(long long n);
 
+// Raises a kernel's dynamic shared-memory limit to the most the device allows
+// it (the opt-in maximum less its static shared memory), once per process and
+// kernel, under a lock: later calls change nothing, so no thread alters a
+// kernel's attribute while another launches it (solvers are created and driven
+// from several host threads).  TP3D_ERR_ARG if `bytes` exceeds that limit.
+int ensure_dynamic_smem(const void* func, int bytes);
+template <typename... P>
+inline int ensure_dynamic_smem(void (*func)(P...), size_t bytes) {
+  return ensure_dynamic_smem(reinterpret_cast<const void*>(func), (int)bytes);
+}
+
 }  // namespace tp3d
 
 #define TP3D_CHECK(expr)                            \

@@ -156,7 +156,7 @@ int check_grid(int nx, int ny, int nz) {
 template <class K>
 int launch_filter(K kernel, const Grid& g, int Z, cudaStream_t st) {
   const size_t smem = filter_smem_bytes(Z);
-  TP3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (int rc = ensure_dynamic_smem(kernel, smem)) return rc;
   (void)st;
   return TP3D_OK;
 }

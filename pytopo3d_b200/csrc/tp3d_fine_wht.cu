@@ -58,15 +58,10 @@ void* wht_fn(int mode, int v) {
 // dynamic shared memory of every instantiation raised once to what it needs
 template <typename T, class ESrc>
 bool wht_prepare(int v) {
-  static bool done[kWhtVariants] = {};
-  if (done[v]) return true;
   const int nthr = WhtShapes<T>::nthr[v];
   const int smem = (int)wht_smem_bytes<T>(nthr);
   for (int mode = 0; mode <= kModeChebStepDot; ++mode)
-    if (cudaFuncSetAttribute(wht_fn<T, ESrc>(mode, v), cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess)
-      return false;
-  done[v] = true;
+    if (ensure_dynamic_smem(wht_fn<T, ESrc>(mode, v), smem) != TP3D_OK) return false;
   return true;
 }
 

@@ -295,7 +295,7 @@ extern "C" int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const d
   const long long ntiles = filter_ntiles(g);
   TP3D_DISPATCH_Z(fc.Z, {
     auto kern = oc_kernel<ZC>;
-    TP3D_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = ensure_dynamic_smem(kern, smem)) return rc;
     int per_sm = 0;
     TP3D_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFilterThreads, smem));
     if (per_sm < 1) {
@@ -467,7 +467,7 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
   const long long ntiles = filter_ntiles(g);
   TP3D_DISPATCH_Z(Z, {
     auto kern = oc_kernel<ZC>;
-    TP3D_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = ensure_dynamic_smem(kern, smem)) return rc;
     int per_sm = 0;
     TP3D_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFilterThreads, smem));
     if (per_sm < 1) {

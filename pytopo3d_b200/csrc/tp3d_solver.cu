@@ -1407,6 +1407,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->deep_cta = 1;
   o->block_sweeps = 0;
   o->resid_restrict_dofs = 0;
+  o->spectra_streams = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1629,11 +1630,9 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     };
     s->deep_inv_smem = bytes(true) <= (size_t)optin;  // the coarsest inverse too, when it fits
     const size_t smem = bytes(s->deep_inv_smem);
-    const cudaError_t e = b16 ? cudaFuncSetAttribute(deep_cycle_kernel<float, __nv_bfloat16>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                              : cudaFuncSetAttribute(deep_cycle_kernel<float, float>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (smem <= (size_t)optin && e == cudaSuccess) {
+    const int e = b16 ? ensure_dynamic_smem(deep_cycle_kernel<float, __nv_bfloat16>, smem)
+                      : ensure_dynamic_smem(deep_cycle_kernel<float, float>, smem);
+    if (e == TP3D_OK) {
       if (b16) s->deep_SN = s->alloc<__nv_bfloat16>((size_t)nn * kDeepRow);
       if (!b16 || s->deep_SN) {
         s->deep_L = L;
@@ -1713,6 +1712,8 @@ static int spectra_level(tp3d_solver* s, int L, cudaStream_t ps) {
 // at the end of the set-up (join_spectra).
 static int fork_spectra(tp3d_solver* s, int L) {
   if (s->o.smoother == 1 || L >= s->nlev - 1 + (s->nlev == 1 ? 1 : 0)) return TP3D_OK;
+  if (!s->o.spectra_streams)  // in order on the solver's stream
+    return s->mixed ? spectra_level<float>(s, L, s->st) : spectra_level<double>(s, L, s->st);
   cudaStream_t ps = s->st_pow[L];
   TP3D_CHECK(cudaEventRecord(s->ev_pow_in[L], s->st));
   TP3D_CHECK(cudaStreamWaitEvent(ps, s->ev_pow_in[L], 0));
@@ -1723,7 +1724,7 @@ static int fork_spectra(tp3d_solver* s, int L) {
 
 static int join_spectra(tp3d_solver* s) {
   if (s->o.smoother == 1) return TP3D_OK;
-  for (int L = 0; L < s->nlev - 1 + (s->nlev == 1 ? 1 : 0); ++L)
+  for (int L = 0; L < s->nlev - 1 + (s->nlev == 1 ? 1 : 0) && s->o.spectra_streams; ++L)
     TP3D_CHECK(cudaStreamWaitEvent(s->st, s->ev_pow_out[L], 0));
   s->have_spectra = true;
   return TP3D_OK;
@@ -1774,8 +1775,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     } else {
       const size_t smem = 2 * (size_t)n * sizeof(double);
       if (smem > 48 * 1024)
-        TP3D_CHECK(cudaFuncSetAttribute(dense_gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
+        if (int rc = ensure_dynamic_smem(dense_gj_inverse_kernel, smem)) return rc;
       dense_gj_inverse_kernel<<<1, 1024, smem, cs>>>(n, s->cdense, s->cinv64, 0, s->cstatus);
       count_launch();
     }
