@@ -12,11 +12,13 @@
 // multiplies by the coarsest inverse, prolongs and smooths again, and writes
 // the level's iterate back.  Every phase calls the same per-node device
 // functions and epilogues as the separate kernels, with plain loads from
-// shared memory.  With a bf16 stencil the block reads it node-major (one
-// thread per node computes the node's three rows from 31 16-byte loads and
-// 81 neighbour values, kDeepRow entries per node); rows are summed in partial
-// sums (FP32: one per z-plane of neighbours; bf16: two per row), so they round
-// differently from the separate kernels' single sum.
+// shared memory.  With a bf16 stencil the block reads it node-major: four
+// warps share 32 nodes, warp q of the four reads chunks 8q .. 8q+7 of each
+// node's 31 16-byte chunks (kDeepRow entries per node) and computes the
+// node's three partial rows, and the four partial sums are added in a fixed
+// order after a block barrier.  Rows are summed in partial sums (FP32 stencil:
+// one per z-plane of neighbours), so they round differently from the separate
+// kernels' single sum.
 #pragma once
 
 #include "tp3d_hex.cuh"
@@ -52,10 +54,12 @@ __global__ void deep_pack_kernel(Grid g, const double* __restrict__ A, const uin
   }
 }
 
-// K u at the three DOFs of node n from the node-major bf16 stencil in shared
-// memory, two partial sums per row.
-template <typename T>
-__device__ __forceinline__ void deep_node_rows(const Grid& g, const __nv_bfloat16* SN, const T* u, int n, T y[3]) {
+// Part Q of K u at the three DOFs of node n from the node-major bf16 stencil
+// in shared memory: the entries of chunks 8Q .. 8Q+7.
+constexpr int kDeepPassNodes = 256;  // nodes per pass of the block: 8 groups of 32, four warps per group
+
+template <typename T, int Q>
+__device__ __forceinline__ void deep_node_part(const Grid& g, const __nv_bfloat16* SN, const T* u, int n, T y[3]) {
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const int NXY = NX * NY;
   const int iy = n % NY, r = n / NY;
@@ -66,7 +70,7 @@ __device__ __forceinline__ void deep_node_rows(const Grid& g, const __nv_bfloat1
   const uint4* row = reinterpret_cast<const uint4*>(SN + (size_t)n * kDeepRow);
   T acc[3][2] = {{T(0), T(0)}, {T(0), T(0)}, {T(0), T(0)}};
 #pragma unroll
-  for (int q = 0; q < kDeepRow / 8; ++q) {
+  for (int q = 8 * Q; q < 8 * Q + 8 && q < kDeepRow / 8; ++q) {
     const uint4 w = row[q];
     const unsigned ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
@@ -116,14 +120,15 @@ __host__ __device__ constexpr size_t deep_stencil_bytes(long long nn) {
 
 // Shared-memory bytes of the block for a level of `nn` nodes and a coarsest
 // level of `nnc` nodes: stencil, six level vectors (x[2], b, d, dinv, r), two
-// coarsest vectors, node masks, and with inv_smem the coarsest inverse;
-// 16-byte aligned parts.
+// coarsest vectors, node masks, the four partial rows of a pass (bf16
+// stencil), and with inv_smem the coarsest inverse; 16-byte aligned parts.
 template <typename T, typename TS>
 __host__ __device__ constexpr size_t deep_smem_bytes(long long nn, long long nnc, bool inv_smem) {
   const size_t nd = (size_t)(3 * nn), ndc = (size_t)(3 * nnc);
   auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
   return al(deep_stencil_bytes<TS>(nn)) + 6 * al(nd * sizeof(T)) + 2 * al(ndc * sizeof(T)) + al((size_t)nn) +
-         al((size_t)nnc) + (inv_smem ? al(ndc * ndc * sizeof(T)) : 0);
+         al((size_t)nnc) + (sizeof(TS) == 2 ? al(4 * 3 * kDeepPassNodes * sizeof(T)) : 0) +
+         (inv_smem ? al(ndc * ndc * sizeof(T)) : 0);
 }
 
 // 16-byte asynchronous copies global -> shared of the first (bytes / 16) * 16
@@ -208,6 +213,8 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   q += al((size_t)nn);
   uint8_t* fixc = q;
   q += al((size_t)nnc);
+  T* ypart = reinterpret_cast<T*>(q);  // [4 parts][3 components][kDeepPassNodes]
+  if (kNode) q += al(4 * 3 * kDeepPassNodes * sizeof(T));
   T* inv = p.inv_smem ? reinterpret_cast<T*>(q) : nullptr;
 
   const int t = threadIdx.x;
@@ -225,6 +232,29 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   for (int n = t; n < nnc; n += kDeepThreads) fixc[n] = p.fixc[n];
   deep_copy_wait();
   __syncthreads();
+
+  // K x[cur] of the nodes of pass `base` into ypart (bf16 stencil); the caller
+  // waits at a block barrier before reading it
+  auto node_pass = [&](int base, const T* xv) {
+    const int w = t >> 5, l = t & 31;
+    const int nl = (w >> 2) * 32 + l, qp = w & 3;
+    const int n = base + nl;
+    T y[3] = {T(0), T(0), T(0)};
+    if (n < nn) {
+      const __nv_bfloat16* SN = reinterpret_cast<const __nv_bfloat16*>(S);
+      if (qp == 0) deep_node_part<T, 0>(p.g, SN, xv, n, y);
+      else if (qp == 1) deep_node_part<T, 1>(p.g, SN, xv, n, y);
+      else if (qp == 2) deep_node_part<T, 2>(p.g, SN, xv, n, y);
+      else deep_node_part<T, 3>(p.g, SN, xv, n, y);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ypart[(qp * 3 + c) * kDeepPassNodes + nl] = y[c];
+  };
+  auto node_sum = [&](int nl, int c) {
+    return ((ypart[(0 * 3 + c) * kDeepPassNodes + nl] + ypart[(1 * 3 + c) * kDeepPassNodes + nl]) +
+            ypart[(2 * 3 + c) * kDeepPassNodes + nl]) +
+           ypart[(3 * 3 + c) * kDeepPassNodes + nl];
+  };
 
   int cur = 0;
   auto smooth = [&](int s, bool first) {
@@ -246,11 +276,15 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
       else op_epilogue<T, kModeChebStep>(io, i, fx, kv, own, epi_load<T, kModeChebStep>(io, i), part);
     };
     if constexpr (kNode) {
-      for (int n = t; n < nn; n += kDeepThreads) {
-        T y[3];
-        deep_node_rows<T>(p.g, reinterpret_cast<const __nv_bfloat16*>(S), x[cur], n, y);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) epi(3 * n + c, n, c, y[c]);
+      for (int base = 0; base < nn; base += kDeepPassNodes) {
+        node_pass(base, x[cur]);
+        __syncthreads();
+        const int cnt = 3 * (int)min((long long)kDeepPassNodes, nn - base);
+        for (int k = t; k < cnt; k += kDeepThreads) {
+          const int nl = k / 3, c = k - 3 * nl;
+          epi(3 * (base + nl) + c, base + nl, c, node_sum(nl, c));
+        }
+        __syncthreads();
       }
     } else {
       for (int i = t; i < nd; i += kDeepThreads) {
@@ -266,11 +300,15 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
   for (int s = 1; s < p.pre; ++s) smooth(s, false);
   // residual
   if constexpr (kNode) {
-    for (int n = t; n < nn; n += kDeepThreads) {
-      T y[3];
-      deep_node_rows<T>(p.g, reinterpret_cast<const __nv_bfloat16*>(S), x[cur], n, y);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) r[3 * n + c] = ((fix[n] >> c) & 1) ? T(0) : b[3 * n + c] - y[c];
+    for (int base = 0; base < nn; base += kDeepPassNodes) {
+      node_pass(base, x[cur]);
+      __syncthreads();
+      const int cnt = 3 * (int)min((long long)kDeepPassNodes, nn - base);
+      for (int k = t; k < cnt; k += kDeepThreads) {
+        const int nl = k / 3, c = k - 3 * nl, n = base + nl;
+        r[3 * n + c] = ((fix[n] >> c) & 1) ? T(0) : b[3 * n + c] - node_sum(nl, c);
+      }
+      __syncthreads();
     }
   } else {
     for (int i = t; i < nd; i += kDeepThreads) {

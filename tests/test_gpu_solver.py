@@ -211,11 +211,12 @@ def test_split_stencil_matches_one_thread_per_dof(P, dims, prec):
 # thread's order rather than four lanes'): same iterations within one or 2%,
 # same solution to the mixed form's rounding.  The block holds the level's
 # operator in shared memory, so it is used when that fits: a last smoothed
-# level of at most about 400 nodes with bf16 stencils (64x32x32: 9x5x5 nodes;
-# 40x20x20: 11x6x6; 16x8x8: 9x5x5), not for 48x24x24 (13x7x7), and not with
-# damped Jacobi, whose levels keep FP32 stencils (twice the bytes).
+# level of at most about 380 nodes with bf16 stencils (64x32x32: 9x5x5 nodes;
+# 16x8x8: 9x5x5), not for 40x20x20 (11x6x6 = 396 nodes) or 48x24x24
+# (13x7x7), and not with damped Jacobi, whose levels keep FP32 stencils
+# (twice the bytes).
 @pytest.mark.parametrize("smoother", [0, 1])
-@pytest.mark.parametrize("dims,fits", [((64, 32, 32), True), ((40, 20, 20), True), ((16, 8, 8), True),
+@pytest.mark.parametrize("dims,fits", [((64, 32, 32), True), ((40, 20, 20), False), ((16, 8, 8), True),
                                        ((48, 24, 24), False)])
 def test_deep_block_cycle_matches_per_phase_launches(P, dims, fits, smoother):
     from pytopo3d_b200._tensors import to_flat
