@@ -121,9 +121,12 @@ int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const double* x,
  * loading this library holds until exit; grids above
  * tp3d_oc_noalloc_max_elements() (262144) elements are rejected with
  * TP3D_ERR_ARG.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array, so calls that overlap on the GPU race; issue them
- * on one stream.  Arguments and results are those of tp3d_oc_update. */
+ * (cudaGetSymbolAddress) and should come before any stream capture.  Each
+ * call queues only device work on `stream` (the filter column table is built
+ * in the array by a small kernel, the barrier words and stats are cleared by
+ * memsets): no host buffer is read after the call returns.  All calls share
+ * the array, so calls that overlap on the GPU race; issue them on one stream.
+ * Arguments and results are those of tp3d_oc_update. */
 long long tp3d_oc_noalloc_max_elements(void);
 int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin, const double* x,
                            const double* dc_dx, const double* dv_dx, const double* Hs,
@@ -131,6 +134,48 @@ int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin, const doub
                            double target_free_volume, double beta, double eta, int max_bisection,
                            double bisection_tol, double* x_new, double* rho_new, double* stats,
                            void* stream);
+
+/* Wait-expiry test hook: from the next OC launch on, every grid-barrier wait
+ * of the OC kernel gives up after `spin_limit` polls (0 = the normal limit of
+ * about a second) and waits for `phantom_blocks` extra blocks that never
+ * arrive (0 = none), so with phantom_blocks > 0 every wait runs out and the
+ * launch ends with its stats left NaN, which the Python layer reports as
+ * Topo3dError.  Process-wide; tests only (it checks that an expired bounded
+ * wait reaches the host as an error and leaves the context usable).  No
+ * reference counterpart. */
+int tp3d_debug_expire_oc_waits(long long spin_limit, int phantom_blocks);
+
+/* ---------------------------------------------------------------------------
+ * Obstacle masks
+ * ------------------------------------------------------------------------- */
+
+#define TP3D_OBSTACLE_CUBE 0
+#define TP3D_OBSTACLE_SPHERE 1
+#define TP3D_OBSTACLE_CYLINDER 2
+
+/* One obstacle primitive in element indices (x, y, z order), as the reference
+ * computes them from fractions with int() truncation:
+ *   cube:     lo <= (x, y, z) < hi                    (obstacles.py:12-61)
+ *   sphere:   |(x, y, z) - center|^2 <= r2            (obstacles.py:63-108)
+ *   cylinder: squared distance to center in the two axes other than `axis`
+ *             <= r2, and lo[axis] <= coordinate along axis < hi[axis]
+ *                                                     (obstacles.py:110-193) */
+typedef struct tp3d_obstacle {
+  int kind;
+  int axis;
+  int center[3];
+  int lo[3];
+  int hi[3];
+  long long r2;
+} tp3d_obstacle;
+
+/* mask[e] = 1 where any of the `nshapes` primitives (host array) contains
+ * element e, else 0; mask is a device array of nelx*nely*nelz bytes in the
+ * element order above.  Replaces the numpy mask construction of
+ * create_cube/sphere/cylinder_obstacle and the OR of parse_obstacle_config_file
+ * (pytopo3d/utils/obstacles.py:12-269). */
+int tp3d_obstacle_mask(int nelx, int nely, int nelz, const tp3d_obstacle* shapes, int nshapes, uint8_t* mask,
+                       void* stream);
 
 /* ---------------------------------------------------------------------------
  * Matrix-free H8 elasticity solver (multigrid-preconditioned CG)

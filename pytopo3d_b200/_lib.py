@@ -81,6 +81,8 @@ SIGNATURES = {
     "tp3d_oc_noalloc_max_elements": (i64, []),
     "tp3d_oc_update_noalloc": (i32, [i32, i32, i32, f64, vp, vp, vp, vp, vp, vp, f64, f64, f64, f64, i32, f64, vp,
                                      vp, vp, vp]),
+    "tp3d_debug_expire_oc_waits": (i32, [i64, i32]),
+    "tp3d_obstacle_mask": (i32, [i32, i32, i32, vp, i32, vp, vp]),
     "tp3d_solver_default_opts": (None, [C.POINTER(SolverOpts)]),
     "tp3d_solver_create": (i32, [i32, i32, i32, vp, vp, C.POINTER(SolverOpts), vp, C.POINTER(vp)]),
     "tp3d_solver_destroy": (i32, [vp]),

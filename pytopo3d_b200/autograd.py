@@ -11,8 +11,9 @@ their gradient check (tests/test_projected_optimizer.py:24-80):
   variables (filter.py:103-119).
 
 Both run in the fused ``tp3d_sensitivity`` kernel.  Displacements are kept
-from the forward pass (``recompute=False``), or they are re-solved per load case in
-backward when device memory is short (``recompute=True``).
+from the forward pass on the autograd context (``recompute=False``), or they
+are re-solved per load case in backward when device memory is short
+(``recompute=True``).
 """
 
 from __future__ import annotations
@@ -62,33 +63,42 @@ class ComplianceProblem:
                                    dtype=torch.uint8, device=device())
         self.U = torch.zeros_like(self.F)
 
-    def forward(self, x_flat: torch.Tensor) -> torch.Tensor:
+    def forward(self, x_flat: torch.Tensor, keep: bool = False):
+        """Summed compliance of the flat design; with ``keep`` also the state the
+        adjoint needs (physical density, projection derivative, one displacement
+        field per load case) as fresh tensors owned by the caller."""
         project_flat(self.H, x_flat, self.Hs, self.beta, self.eta, self.solid, self.void, self.rho_f,
                      self.rho_p, self.dproj)
         self.solver.set_density(self.rho_p, self.penal)
         total = torch.zeros((), dtype=torch.float64, device=device())
+        U = torch.zeros_like(self.F) if keep else self.U
         for k in range(self.F.shape[0]):
-            self.U[k].zero_()
-            self.solver.solve(self.F[k], self.U[k])
-            total = total + torch.dot(self.F[k], self.U[k])
-        return total
+            U[k].zero_()
+            self.solver.solve(self.F[k], U[k])
+            total = total + torch.dot(self.F[k], U[k])
+        state = (self.rho_p.clone(), self.dproj.clone(), U) if keep else None
+        return total, state
 
-    def gradient(self, x_flat: torch.Tensor) -> torch.Tensor:
-        """d compliance / d x (flat), reusing or recomputing the displacements."""
+    def gradient(self, x_flat: torch.Tensor, state=None) -> torch.Tensor:
+        """d compliance / d x (flat): from the saved ``state`` of the forward pass,
+        or with the displacements recomputed per load case when ``state`` is None."""
         L = _lib.lib()
         H = self.H
-        if self.recompute:
+        if state is None:
             project_flat(self.H, x_flat, self.Hs, self.beta, self.eta, self.solid, self.void, self.rho_f,
                          self.rho_p, self.dproj)
             self.solver.set_density(self.rho_p, self.penal)
+            rho_p, dproj, U = self.rho_p, self.dproj, self.U
+        else:
+            rho_p, dproj, U = state
         out = torch.zeros(self.nele, dtype=torch.float64, device=device())
         for k in range(self.F.shape[0]):
-            if self.recompute:
-                self.U[k].zero_()
-                self.solver.solve(self.F[k], self.U[k])
+            if state is None:
+                U[k].zero_()
+                self.solver.solve(self.F[k], U[k])
             _lib.check(L.tp3d_sensitivity(
-                H.nelx, H.nely, H.nelz, H.rmin, self.U[k].data_ptr(), self.KE.ctypes.data,
-                self.rho_p.data_ptr(), self.dproj.data_ptr(), self.Hs.data_ptr(), self.free.data_ptr(),
+                H.nelx, H.nely, H.nelz, H.rmin, U[k].data_ptr(), self.KE.ctypes.data,
+                rho_p.data_ptr(), dproj.data_ptr(), self.Hs.data_ptr(), self.free.data_ptr(),
                 self.penal, self.ce.data_ptr(), self.dc.data_ptr(), self.dv.data_ptr(), self.c.data_ptr(),
                 self.scratch.data_ptr(), _lib.stream_ptr()), "sensitivity")
             out += self.dc
@@ -99,20 +109,31 @@ class ComplianceProblem:
 
 
 class _Compliance(torch.autograd.Function):
+    """The forward pass's state lives on ``ctx``: with ``recompute=False`` each
+    call saves its own physical density, projection derivative and
+    displacements, so several forwards before their backwards each get the
+    gradient of their own design.  With ``recompute=True`` only the design is
+    saved and backward re-solves every load case."""
+
     @staticmethod
     def forward(ctx, rho_design: torch.Tensor, problem: ComplianceProblem):
         x = rho_design.detach()
         shape = tuple(x.shape)
         xf = x.permute(2, 1, 0).contiguous().reshape(-1) if x.dim() == 3 else x.contiguous()
-        c = problem.forward(xf.to(torch.float64))
+        xf = xf.to(torch.float64)
+        c, state = problem.forward(xf, keep=not problem.recompute)
         ctx.problem, ctx.shape, ctx.dim = problem, shape, x.dim()
-        ctx.save_for_backward(xf)
+        if state is None:
+            ctx.save_for_backward(xf)
+        else:
+            ctx.save_for_backward(xf, *state)
         return c.to(rho_design.dtype)
 
     @staticmethod
     def backward(ctx, grad_out):
-        (xf,) = ctx.saved_tensors
-        g = ctx.problem.gradient(xf) * grad_out.to(torch.float64)
+        saved = ctx.saved_tensors
+        state = None if len(saved) == 1 else tuple(saved[1:])
+        g = ctx.problem.gradient(saved[0], state) * grad_out.to(torch.float64)
         if ctx.dim == 3:
             g = from_flat(g, ctx.shape)
         return g, None

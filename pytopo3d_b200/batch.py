@@ -27,7 +27,8 @@ import torch
 
 from ._tensors import device
 from .assembly import build_force_vector, build_supports
-from .obstacles import cylinder_mask_elements
+from ._tensors import to_flat_mask
+from .obstacles import cylinder_elements, obstacle_mask_flat
 from .optimizer import SimpLoop, _elements_at_loaded_nodes
 from .stiffness import lk_H8
 
@@ -76,20 +77,21 @@ def design_problem(spec: DesignSpec):
     """Masks, total-unit load, fixed DOFs of one design: clamped at x = 0, the
     -z load on the chosen x = nelx edge; elements at the clamped face and at the
     loaded nodes are protected solid (optimizer.py:366-390), void wins over
-    solid (:392-399)."""
+    solid (:392-399).  The masks are flat uint8 device tensors: the void
+    cylinders are built by the obstacle-mask kernel on the current stream."""
     nelx, nely, nelz = spec.nelx, spec.nely, spec.nelz
     shape = (nely, nelx, nelz)
+    dims = (nelx, nely, nelz)
     ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
-    void = np.zeros(shape, bool)
-    for axis, ca, cb, r in spec.cylinders:
-        void |= cylinder_mask_elements(shape, ca, cb, r, axis)
+    void = obstacle_mask_flat(shape, [cylinder_elements(axis, ca, cb, r, dims[axis])
+                                      for axis, ca, cb, r in spec.cylinders])
     F = np.zeros(ndof)
     iz = nelz // 2 if spec.load_mid else 0
     for iy in range(nely + 1):
         F[3 * (iy + (nely + 1) * (nelx + (nelx + 1) * iz)) + 2] = -1.0 / (nely + 1)
     solid = _elements_at_loaded_nodes(F[None, :], nelx, nely, nelz)
     solid[:, 0, :] = True
-    solid &= ~void
+    solid = to_flat_mask(solid) & (void == 0).to(torch.uint8)
     free, _ = build_supports(nelx, nely, nelz, ndof)
     fixed = np.ones(ndof, np.uint8)
     fixed[free] = 0

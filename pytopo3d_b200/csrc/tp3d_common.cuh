@@ -94,11 +94,12 @@ __device__ __forceinline__ double sum_partials(const double* p, int n, double* s
 
 // ---------------------------------------------------------------------------
 // Grid-wide barrier for cooperative (co-resident) launches.  The spin is
-// bounded: after `kSpinLimit` polls the barrier gives up, raises `*err` and
-// returns false so that every block can leave its loop and the host reads a
-// status instead of the GPU hanging.
+// bounded: after `kSpinLimit` polls (with the back-off of the waits below,
+// about a second) the barrier gives up, raises `*err` and returns false so
+// that every block can leave its loop and the host reads a status instead of
+// the GPU hanging.
 // ---------------------------------------------------------------------------
-constexpr long long kSpinLimit = 1ll << 26;
+constexpr long long kSpinLimit = 1ll << 23;
 
 struct GridBarrier {
   unsigned int* count;       // arrivals in the current generation
@@ -142,24 +143,31 @@ __device__ __forceinline__ bool grid_sync(GridBarrier b) {
 // last block arrives, and each block waits for the flip of the value it saw.
 // The word returns to its low bits after every barrier, so it needs no reset
 // between barriers or launches (only a zero before the first launch, and
-// after an expired wait).  Bounded like grid_sync: after kSpinLimit polls the
-// wait raises *err and returns false.
-__device__ __forceinline__ bool grid_sync_flip(unsigned int* word, int* err) {
+// after an expired wait).  Bounded: the wait polls without sleeping for its
+// first 64 polls (the common case, a few microseconds), then backs off with
+// __nanosleep; after `limit` polls (kSpinLimit: about a second) it raises *err
+// and returns false, and every other block leaves at its next poll.
+// `phantom` counts blocks that never arrive: with phantom > 0 the word can
+// never flip, so every wait runs out.  Only the wait-expiry test sets it (with
+// a short limit), to check that an expired wait reaches the host as an error.
+__device__ __forceinline__ bool grid_sync_flip(unsigned int* word, int* err, long long limit = kSpinLimit,
+                                               unsigned int phantom = 0) {
   __syncthreads();
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    const unsigned int nblk = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int nblk = gridDim.x * gridDim.y * gridDim.z + phantom;
     const unsigned int inc = (blockIdx.x | blockIdx.y | blockIdx.z) == 0 ? 0x80000000u - (nblk - 1) : 1u;
     __threadfence();
     const unsigned int seen = atomicAdd(word, inc);
     int ok = 1;
     long long spins = 0;
     while (((seen ^ *(volatile unsigned int*)word) & 0x80000000u) == 0) {
-      if (++spins > kSpinLimit || *(volatile int*)err != 0) {
+      if (++spins > limit || *(volatile int*)err != 0) {
         atomicExch(err, TP3D_ERR_TIMEOUT);
         ok = 0;
         break;
       }
+      if (spins > 64) __nanosleep(64);
     }
     __threadfence();
     s_ok = ok;

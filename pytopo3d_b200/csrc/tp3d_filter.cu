@@ -36,33 +36,16 @@ int filter_cols_for(double rmin, FilterCols* out) {
   auto key = std::make_pair(dev, bits);
   auto it = g_cols.find(key);
   if (it == g_cols.end()) {
-    const int R = (int)std::ceil(rmin) + 1;
-    int Z = 0;
-    for (int d = 0; d <= R; ++d)
-      if (rmin - std::sqrt((double)(d * d)) > 1e-9) Z = d;
+    const int Z = filter_radius_z(rmin);
+    if (Z < 0) return TP3D_ERR_ARG;
     if (Z > kFilterMaxZ) {
       tp3d_set_last_error("rmin too large for the stencil filter (max 7)");
       return TP3D_ERR_ARG;
     }
-    const int W = 2 * Z + 1;
-    std::vector<int2> dxy;
-    std::vector<double> w;
-    for (int dx = -Z; dx <= Z; ++dx)
-      for (int dy = -Z; dy <= Z; ++dy) {
-        std::vector<double> col(W, 0.0);
-        bool any = false;
-        for (int dz = -Z; dz <= Z; ++dz) {
-          const double wt = rmin - std::sqrt((double)(dx * dx + dy * dy + dz * dz));
-          if (wt > 1e-9) {
-            col[dz + Z] = wt;
-            any = true;
-          }
-        }
-        if (any) {
-          dxy.push_back(make_int2(dx, dy));
-          w.insert(w.end(), col.begin(), col.end());
-        }
-      }
+    const int ncols = filter_columns_build(rmin, Z, nullptr, nullptr);
+    std::vector<int2> dxy(ncols);
+    std::vector<double> w((size_t)ncols * (2 * Z + 1));
+    filter_columns_build(rmin, Z, dxy.data(), w.data());
     ColsEntry e;
     e.ncols = (int)dxy.size();
     e.Z = Z;

@@ -18,7 +18,7 @@ constexpr int kFilterTY = 32;   // outputs along y per block (one warp)
 constexpr int kFilterTX = 8;    // outputs along x per block (warps per block)
 constexpr int kFilterKZ = 8;    // outputs along z per thread
 constexpr int kFilterThreads = kFilterTY * kFilterTX;
-constexpr int kFilterMaxZ = 6;  // supports rmin <= 7
+constexpr int kFilterMaxZ = 6;  // supports rmin <= 7 (the staged tile of Z = 7 exceeds shared memory)
 
 struct FilterCols {
   const int2* dxy;    // (dx, dy) per column
@@ -29,6 +29,55 @@ struct FilterCols {
 
 // Host: columns for a radius, cached per (device, rmin).  Returns nonzero on error.
 int filter_cols_for(double rmin, FilterCols* out);
+
+// Largest offset along one axis with a positive cone weight: the largest d with
+// rmin - d > 1e-9 (pytopo3d/utils/filter.py:193-206).  -1 for an invalid rmin.
+__host__ __device__ inline int filter_radius_z(double rmin) {
+  if (!(rmin > 0.0) || !(rmin < 1.0e6)) return -1;
+  int Z = 0;
+  for (int d = 1; d <= (int)rmin + 1; ++d)
+    if (rmin - sqrt((double)(d * d)) > 1e-9) Z = d;
+  return Z;
+}
+
+// Column i of the (2Z+1)^2 candidate columns of a radius with max offset Z,
+// in row-major order over (dx, dy) in [-Z, Z]^2: writes its 2Z+1 weights along
+// dz (rmin - sqrt(dx^2 + dy^2 + dz^2) where that exceeds 1e-9, else 0) and
+// returns whether it has any tap (pytopo3d/utils/filter.py:193-206).
+__host__ __device__ inline bool filter_column(double rmin, int Z, int i, double* wcol) {
+  const int W = 2 * Z + 1;
+  const int dx = i / W - Z, dy = i % W - Z;
+  bool any = false;
+  for (int dz = -Z; dz <= Z; ++dz) {
+    const double wt = rmin - sqrt((double)(dx * dx + dy * dy + dz * dz));
+    const bool tap = wt > 1e-9;
+    any = any || tap;
+    wcol[dz + Z] = tap ? wt : 0.0;
+  }
+  return any;
+}
+
+// The column table of a radius with max offset Z <= kFilterMaxZ: the columns
+// of filter_column that have a tap, in that order, with their (dx, dy)
+// offsets.  Returns the number of columns; dxy / w may be null (count only).
+// The host builds the cached tables with it, and the allocation-free OC path
+// builds its table on the device from filter_column in the same order, so
+// both give the same columns and bit-identical weights (IEEE sqrt and
+// subtraction on both sides).
+__host__ __device__ inline int filter_columns_build(double rmin, int Z, int2* dxy, double* w) {
+  const int W = 2 * Z + 1;
+  int n = 0;
+  for (int i = 0; i < W * W; ++i) {
+    double col[2 * kFilterMaxZ + 1];
+    if (filter_column(rmin, Z, i, col)) {
+      if (dxy) dxy[n] = make_int2(i / W - Z, i % W - Z);
+      if (w)
+        for (int j = 0; j < W; ++j) w[(size_t)n * W + j] = col[j];
+      ++n;
+    }
+  }
+  return n;
+}
 
 __host__ __device__ inline int filter_smem_elems(int Z) {
   return (kFilterTY + 2 * Z) * (kFilterTX + 2 * Z) * (kFilterKZ + 2 * Z);

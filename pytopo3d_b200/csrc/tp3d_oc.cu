@@ -10,10 +10,10 @@
 // fixed order after a (bounded) grid barrier, so every block takes the same
 // bisection decision.  Only the best multiplier is kept; the best candidate is
 // recomputed from it at the end, so no candidate array is stored.
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <mutex>
-#include <vector>
 
 #include "tp3d_filter.cuh"
 
@@ -42,7 +42,19 @@ struct OcArgs {
   double* partB;     // kOcMaxBlocks
   double* partC;     // kOcMaxBlocks
   GridBarrier bar;
+  long long spin_limit;   // polls before a grid-barrier wait gives up
+  unsigned int phantom;   // blocks the barrier waits for that never arrive (wait-expiry test only)
 };
+
+// Wait-expiry test hook (tp3d_debug_expire_oc_waits): 0 = normal waits.
+std::atomic<long long> g_test_spin_limit{0};
+std::atomic<int> g_test_phantom{0};
+
+void set_wait_policy(OcArgs& a) {
+  const long long lim = g_test_spin_limit.load();
+  a.spin_limit = lim > 0 ? lim : kSpinLimit;
+  a.phantom = (unsigned int)g_test_phantom.load();
+}
 
 // Per-element code written once per call into the ratio scratch: for a free
 // element q = sqrt(normalised ratio) >= 0; -1 marks protected solid, -2
@@ -93,7 +105,7 @@ __device__ bool oc_volume(const OcArgs& a, double lam, double* part, double* s, 
   }
   vpart = block_sum(vpart, red);
   if (threadIdx.x == 0) part[blockIdx.x] = vpart;
-  if (!grid_sync_flip(a.bar.count, a.bar.err)) return false;
+  if (!grid_sync_flip(a.bar.count, a.bar.err, a.spin_limit, a.phantom)) return false;
   *vol = sum_partials(part, gridDim.x, red);
   return true;
 }
@@ -120,7 +132,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   }
   m = block_max(m, red);
   if (threadIdx.x == 0) a.partC[blockIdx.x] = m;
-  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err, a.spin_limit, a.phantom)) return;
   double scale = 0.0;
   {
     double t = 0.0;
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
     else q = sqrt(scale > 0.0 ? a.ratio[e] / scale : 1.0);
     a.ratio[e] = q;
   }
-  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err, a.spin_limit, a.phantom)) return;
 
   // ---- bisection (oc_update.py:70-122) ----
   // The reference starts from [0, 1e12]; while the projected volume stays at or
@@ -165,24 +177,65 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   if (a.tol < 1.0) {
     int jlo = 0, jhi = a.max_iter + 1;
     double vlo = NAN, vhi = NAN;
+    constexpr int kProbes = 16;  // the search over j <= 81 makes at most 8 probes
+    int pj[kProbes];
+    double pv[kProbes];
+    int np = 0;
     bool first = true;  // probe j = 1 first: it is the reference's own first step, and K = 0 is common
+    auto eval_j = [&](int j, double* v) {
+      return oc_volume<Z>(a, ldexp(1.0e12, -j), (pass++ & 1) ? a.partB : a.partA, s, red, v);
+    };
     while (jhi - jlo > 1) {
       const int jm = first ? 1 : (jlo + jhi) >> 1;
       first = false;
       double v;
-      if (!oc_volume<Z>(a, ldexp(1.0e12, -jm), (pass++ & 1) ? a.partB : a.partA, s, red, &v)) return;
+      if (!eval_j(jm, &v)) return;
       if (v > a.target) {
         jhi = jm;
         vhi = v;
       } else {
         jlo = jm;
         vlo = v;
+        if (np < kProbes) {
+          pj[np] = jm;
+          pv[np] = v;
+          ++np;
+        }
       }
     }
-    if (jlo >= 1) {  // steps 1..jlo: only the best of them (step jlo) is recorded
-      it = jlo - 1;
-      hi = ldexp(1.0e12, -(jlo - 1));
-      record(ldexp(1.0e12, -jlo), vlo);
+    if (jlo >= 1) {
+      // Steps 1..K (K = jlo) only halve the upper bound, and their volumes do
+      // not decrease with j, so the smallest error among them is step K's.
+      // The reference keeps the FIRST step with the smallest error (strict <,
+      // oc_update.py:106): if steps before K have exactly step K's volume (a
+      // plateau, e.g. every candidate held at its move limit), it reports the
+      // first of them.  Those steps form a range j0..K; j0 is found from the
+      // probes (jb: largest probe below K with a smaller volume, jeq: smallest
+      // probe with step K's volume), evaluating step K - 1 when no probe
+      // decides it and bisecting (jb, jeq] only when a tie is seen.
+      int jb = 0, jeq = jlo;
+      for (int i = 0; i < np; ++i) {
+        if (pv[i] < vlo) jb = max(jb, pj[i]);
+        else if (pv[i] == vlo) jeq = min(jeq, pj[i]);
+      }
+      if (jeq == jlo && jb < jlo - 1) {
+        double v;
+        if (!eval_j(jlo - 1, &v)) return;
+        if (v == vlo) jeq = jlo - 1;
+        else jb = jlo - 1;
+      }
+      while (jeq - jb > 1) {
+        const int jm = (jb + jeq) >> 1;
+        double v;
+        if (!eval_j(jm, &v)) return;
+        if (v == vlo) jeq = jm;
+        else jb = jm;
+      }
+      best_err = fabs(vlo - a.target);
+      best_lam = ldexp(1.0e12, -jeq);
+      best_vol = vlo;
+      hi = ldexp(1.0e12, -jlo);
+      it = jlo;
     }
     if (jhi <= a.max_iter && !done) record(ldexp(1.0e12, -jhi), vhi);  // = 0.5 (lo + hi)
   }
@@ -205,7 +258,7 @@ __global__ void __launch_bounds__(kFilterThreads) oc_kernel(OcArgs a) {
   }
   cmax = block_max(cmax, red);
   if (threadIdx.x == 0) a.partC[blockIdx.x] = cmax;
-  if (!grid_sync_flip(a.bar.count, a.bar.err)) return;
+  if (!grid_sync_flip(a.bar.count, a.bar.err, a.spin_limit, a.phantom)) return;
   for (long long t = blockIdx.x; t < ntiles; t += nblk) {
     const FilterTile tile = filter_tile_at(a.g, t);
     __syncthreads();
@@ -275,6 +328,7 @@ extern "C" int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const d
 
   OcArgs a{g, fc, x, dc_dx, dv_dx, Hs, solid, void_, move, target_free_volume, bisection_tol,
            max_bisection, Projection(beta, eta), x_new, rho_new, stats};
+  set_wait_policy(a);
   double* base = (double*)scratch;
   a.ratio = base;
   a.partA = base + n;
@@ -323,7 +377,7 @@ extern "C" int tp3d_oc_update(int nelx, int nely, int nelz, double rmin, const d
 // file-scope __device__ array instead.  Every GPU that loads this library
 // holds that array (about 2.2 MB) until the process exits.
 // ---------------------------------------------------------------------------
-namespace {
+namespace tp3d_oc_noalloc {
 
 constexpr long long kNoAllocMaxElements = 1LL << 18;  // e.g. 64x64x64 or 128x64x32
 constexpr int kNoAllocMaxCols = (2 * kFilterMaxZ + 1) * (2 * kFilterMaxZ + 1);
@@ -363,40 +417,28 @@ int noalloc_scratch(void** out) {
   return TP3D_OK;
 }
 
-// Filter columns for rmin, built on the host in the same order as the
-// allocating path's table (rmin - |d| > 1e-9, grouped by (dx, dy)).
-int noalloc_columns(double rmin, int* Z, std::vector<int2>* dxy, std::vector<double>* w) {
-  if (!(rmin > 0.0) || !std::isfinite(rmin)) return TP3D_ERR_ARG;
-  const int R = (int)std::ceil(rmin) + 1;
-  int z = 0;
-  for (int d = 0; d <= R; ++d)
-    if (rmin - std::sqrt((double)(d * d)) > 1e-9) z = d;
-  if (z > kFilterMaxZ) {
-    tp3d_set_last_error("rmin too large for the stencil filter (max 7)");
-    return TP3D_ERR_ARG;
+// The filter column table of a radius, built in place in the static scratch:
+// thread i evaluates candidate column i (filter_column, the same function and
+// order as the host-built tables of the allocating path) and writes it at its
+// rank among the columns that have a tap.  No host buffer is involved.
+__global__ void __launch_bounds__(256) noalloc_columns_kernel(double rmin, int Z, int2* dxy, double* w) {
+  __shared__ int has_tap[256];
+  const int W = 2 * Z + 1, i = threadIdx.x;
+  double col[2 * kFilterMaxZ + 1];
+  const bool any = i < W * W && filter_column(rmin, Z, i, col);
+  has_tap[i] = any ? 1 : 0;
+  __syncthreads();
+  if (any) {
+    int pos = 0;
+    for (int k = 0; k < i; ++k) pos += has_tap[k];
+    dxy[pos] = make_int2(i / W - Z, i % W - Z);
+    for (int j = 0; j < W; ++j) w[(size_t)pos * W + j] = col[j];
   }
-  const int W = 2 * z + 1;
-  for (int dx = -z; dx <= z; ++dx)
-    for (int dy = -z; dy <= z; ++dy) {
-      std::vector<double> col(W, 0.0);
-      bool any = false;
-      for (int dz = -z; dz <= z; ++dz) {
-        const double wt = rmin - std::sqrt((double)(dx * dx + dy * dy + dz * dz));
-        if (wt > 1e-9) {
-          col[dz + z] = wt;
-          any = true;
-        }
-      }
-      if (any) {
-        dxy->push_back(make_int2(dx, dy));
-        w->insert(w->end(), col.begin(), col.end());
-      }
-    }
-  *Z = z;
-  return TP3D_OK;
 }
+static_assert((2 * kFilterMaxZ + 1) * (2 * kFilterMaxZ + 1) <= 256, "one thread per candidate column");
 
-}  // namespace
+}  // namespace tp3d_oc_noalloc
+using namespace tp3d_oc_noalloc;
 
 extern "C" long long tp3d_oc_noalloc_max_elements(void) { return kNoAllocMaxElements; }
 
@@ -427,10 +469,12 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
     tp3d_set_last_error("invalid projection parameters");
     return TP3D_ERR_ARG;
   }
-  int Z = 0;
-  std::vector<int2> dxy;
-  std::vector<double> w;
-  if (int rc = noalloc_columns(rmin, &Z, &dxy, &w)) return rc;
+  const int Z = filter_radius_z(rmin);
+  if (Z < 0 || !std::isfinite(rmin)) return TP3D_ERR_ARG;
+  if (Z > kFilterMaxZ) {
+    tp3d_set_last_error("rmin too large for the stencil filter (max 7)");
+    return TP3D_ERR_ARG;
+  }
   void* base_v = nullptr;
   if (int rc = noalloc_scratch(&base_v)) return rc;
   unsigned char* base = (unsigned char*)base_v;
@@ -439,6 +483,7 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
   const Grid g{nelx, nely, nelz};
   OcArgs a{g, FilterCols{}, x, dc_dx, dv_dx, Hs, solid, void_, move, target_free_volume, bisection_tol,
            max_bisection, Projection(beta, eta), x_new, rho_new, stats};
+  set_wait_policy(a);
   a.ratio = (double*)base;
   a.partA = (double*)(base + kNoAllocRatioBytes);
   a.partB = a.partA + kOcMaxBlocks;
@@ -451,12 +496,12 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
   double* d_w = (double*)((unsigned char*)d_dxy + kNoAllocDxyBytes);
   a.fc.dxy = d_dxy;
   a.fc.w = d_w;
-  a.fc.ncols = (int)dxy.size();
+  a.fc.ncols = filter_columns_build(rmin, Z, nullptr, nullptr);  // count only
   a.fc.Z = Z;
   // The array keeps the previous call's contents: the column table is
-  // rewritten and the barrier counters cleared on every call.
-  TP3D_CHECK(cudaMemcpyAsync(d_dxy, dxy.data(), dxy.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-  TP3D_CHECK(cudaMemcpyAsync(d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  // rebuilt on the device and the barrier counters cleared on every call.
+  noalloc_columns_kernel<<<1, 256, 0, st>>>(rmin, Z, d_dxy, d_w);
+  TP3D_CHECK_LAUNCH();
   TP3D_CHECK(cudaMemsetAsync(bar, 0, kNoAllocBarrierBytes, st));
   TP3D_CHECK(cudaMemsetAsync(stats, 0xff, 8 * sizeof(double), st));
 
@@ -480,6 +525,13 @@ extern "C" int tp3d_oc_update_noalloc(int nelx, int nely, int nelz, double rmin,
     TP3D_CHECK(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)grid), dim3(kFilterThreads), args,
                                            smem, st));
   });
-  add_launches(1);
+  add_launches(2);
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_debug_expire_oc_waits(long long spin_limit, int phantom_blocks) {
+  if (spin_limit < 0 || phantom_blocks < 0 || phantom_blocks > 1024) return TP3D_ERR_ARG;
+  g_test_spin_limit.store(spin_limit);
+  g_test_phantom.store(phantom_blocks);
   return TP3D_OK;
 }

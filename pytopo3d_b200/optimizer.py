@@ -10,7 +10,8 @@ plus the logging metrics.
 Extensions (keyword-only): ``F`` — an explicit nodal load vector, or a 2-D
 array of load cases whose compliances are summed; ``precision`` — "fp64"
 (default) or "mixed"; ``solver_options`` — HexSolver options;
-``record`` — a list receiving per-iteration stats.
+``record`` — a list receiving per-iteration stats (and the iteration's new
+design as a flat device tensor, key ``x``).
 """
 
 from __future__ import annotations
@@ -60,6 +61,59 @@ def _elements_at_loaded_nodes(F2, nelx, nely, nelz):
 def _ke(material_params, elem_size):
     return lk_H8(elem_size=elem_size) if material_params is None else lk_H8(*material_params,
                                                                               elem_size=elem_size)
+
+
+def resolve_masks(nelx, nely, nelz, obstacle_mask=None, protected_zone_mask=None, force_field=None,
+                  support_mask=None, F=None):
+    """Protected-solid, protected-void and free masks of a run (optimizer.py:346-405).
+
+    Same precedence, validation messages and warning as the reference: the
+    default load strip ``[:, -1, 0]`` (or the elements carrying a non-zero
+    force field) and the support elements (or the ``x = 0`` face when no or an
+    empty support mask is given) are protected solid; a protected-void element
+    wins where the two overlap.  With an explicit nodal ``F`` (an extension of
+    this package) the elements touching a loaded node take the place of the
+    default load strip.  Returns ``(solid, void, free)`` boolean
+    ``(nely, nelx, nelz)`` arrays; raises ``ValueError`` when no element is free.
+    """
+    expected_shape = (nely, nelx, nelz)
+    obstacle_mask = (np.zeros(expected_shape, dtype=bool) if obstacle_mask is None
+                     else np.asarray(obstacle_mask, dtype=bool).copy())
+    protected_zone_mask = (np.zeros(expected_shape, dtype=bool) if protected_zone_mask is None
+                           else np.asarray(protected_zone_mask, dtype=bool).copy())
+    if obstacle_mask.shape != expected_shape:
+        raise ValueError(f"obstacle_mask has shape {obstacle_mask.shape}, expected {expected_shape}")
+    if protected_zone_mask.shape != expected_shape:
+        raise ValueError("protected_zone_mask has shape "
+                         f"{protected_zone_mask.shape}, expected {expected_shape}")
+    if force_field is None:
+        if F is None:
+            protected_zone_mask[:, -1, 0] = True
+        else:
+            protected_zone_mask |= _elements_at_loaded_nodes(np.atleast_2d(F), nelx, nely, nelz)
+    else:
+        if force_field.shape != expected_shape + (3,):
+            raise ValueError(f"force_field has shape {force_field.shape}, "
+                             f"expected {expected_shape + (3,)}")
+        protected_zone_mask |= np.any(force_field != 0.0, axis=-1)
+    if support_mask is None:
+        protected_zone_mask[:, 0, :] = True
+    else:
+        if support_mask.shape != expected_shape:
+            raise ValueError(f"support_mask has shape {support_mask.shape}, expected {expected_shape}")
+        if np.any(support_mask):
+            protected_zone_mask |= np.asarray(support_mask, dtype=bool)
+        else:
+            protected_zone_mask[:, 0, :] = True
+    overlap = obstacle_mask & protected_zone_mask
+    if np.any(overlap):
+        logger.warning("Protected-solid and protected-void masks overlap at %d elements; "
+                       "protected void takes precedence.", int(np.sum(overlap)))
+        protected_zone_mask[overlap] = False
+    free_mask = ~(obstacle_mask | protected_zone_mask)
+    if not np.any(free_mask):
+        raise ValueError("optimization requires at least one free design element")
+    return protected_zone_mask, obstacle_mask, free_mask
 
 
 class SimpState:
@@ -144,23 +198,32 @@ class SimpLoop:
                  protected_void, projection_eta=0.5, move=0.2, precision="fp64", solver_options=None,
                  x0=None):
         self.shape = (nely, nelx, nelz)
-        solid = np.asarray(protected_solid, bool)
-        void = np.asarray(protected_void, bool)
-        free = ~(solid | void)
-        self.free_host = free
-        self.target = float(volfrac * int(free.sum()))
+        if isinstance(protected_solid, torch.Tensor) or isinstance(protected_void, torch.Tensor):
+            # flat uint8 device masks (Fortran element order), e.g. built by obstacle_mask_flat
+            solid_d = torch.as_tensor(protected_solid).to(device(), torch.uint8).reshape(-1)
+            void_d = torch.as_tensor(protected_void).to(device(), torch.uint8).reshape(-1)
+            free_d = ((solid_d | void_d) == 0).to(torch.uint8)
+            nfree = int(free_d.sum())
+        else:
+            solid = np.asarray(protected_solid, bool)
+            void = np.asarray(protected_void, bool)
+            solid_d, void_d, free_d = to_flat_mask(solid), to_flat_mask(void), to_flat_mask(~(solid | void))
+            nfree = int((~(solid | void)).sum())
+        self.target = float(volfrac * nfree)
         self.eta, self.move, self.penal = float(projection_eta), float(move), float(penal)
         H, Hs = build_filter(nelx, nely, nelz, rmin)
         self.solver = HexSolver(nelx, nely, nelz, KE, fixed_dofs, precision=precision,
                                 **(solver_options or {}))
         Fd = torch.as_tensor(np.atleast_2d(np.asarray(F, dtype=np.float64))).to(device()).contiguous()
-        self.S = SimpState(H, Hs, to_flat_mask(solid), to_flat_mask(void), to_flat_mask(free), KE, Fd,
-                           self.solver, penal)
+        self.S = SimpState(H, Hs, solid_d, void_d, free_d, KE, Fd, self.solver, penal)
         if x0 is None:
-            x0 = np.full(self.shape, volfrac, dtype=float)
-            x0[solid] = 1.0
-            x0[void] = 0.0
-        self.x = to_flat(x0)
+            # volfrac on free elements, 1 on protected solid, 0 on protected void (void wins)
+            x = torch.full((nelx * nely * nelz,), float(volfrac), dtype=torch.float64, device=device())
+            x[solid_d.bool()] = 1.0
+            x[void_d.bool()] = 0.0
+            self.x = x
+        else:
+            self.x = to_flat(x0)
         self.beta = None
         self.last = {}
         n = self.x.numel()
@@ -274,54 +337,20 @@ def top3d(
     if any(not np.isfinite(b) or b <= 0.0 for b in beta_schedule):
         raise ValueError(f"all beta_schedule values must be finite and positive, got {beta_schedule}")
 
-    # ---- masks (optimizer.py:346-405) ----
-    obstacle_mask = (np.zeros(expected_shape, dtype=bool) if obstacle_mask is None
-                     else np.asarray(obstacle_mask, dtype=bool).copy())
-    protected_zone_mask = (np.zeros(expected_shape, dtype=bool) if protected_zone_mask is None
-                           else np.asarray(protected_zone_mask, dtype=bool).copy())
-    if obstacle_mask.shape != expected_shape:
-        raise ValueError(f"obstacle_mask has shape {obstacle_mask.shape}, expected {expected_shape}")
-    if protected_zone_mask.shape != expected_shape:
-        raise ValueError("protected_zone_mask has shape "
-                         f"{protected_zone_mask.shape}, expected {expected_shape}")
-    if force_field is None:
-        if F is None:
-            protected_zone_mask[:, -1, 0] = True
-        else:
-            protected_zone_mask |= _elements_at_loaded_nodes(np.atleast_2d(F), nelx, nely, nelz)
-    else:
-        if force_field.shape != expected_shape + (3,):
-            raise ValueError(f"force_field has shape {force_field.shape}, "
-                             f"expected {expected_shape + (3,)}")
-        protected_zone_mask |= np.any(force_field != 0.0, axis=-1)
-    if support_mask is None:
-        protected_zone_mask[:, 0, :] = True
-    else:
-        if support_mask.shape != expected_shape:
-            raise ValueError(f"support_mask has shape {support_mask.shape}, expected {expected_shape}")
-        if np.any(support_mask):
-            protected_zone_mask |= np.asarray(support_mask, dtype=bool)
-        else:
-            protected_zone_mask[:, 0, :] = True
-    overlap = obstacle_mask & protected_zone_mask
-    if np.any(overlap):
-        logger.warning("Protected-solid and protected-void masks overlap at %d elements; "
-                       "protected void takes precedence.", int(np.sum(overlap)))
-        protected_zone_mask[overlap] = False
-    free_mask = ~(obstacle_mask | protected_zone_mask)
-    design_nele = int(np.sum(free_mask))
-    if design_nele == 0:
-        raise ValueError("optimization requires at least one free design element")
-    target_free_volume = float(volfrac * design_nele)
     ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    if F is not None:
+        F = np.atleast_2d(np.asarray(F, dtype=np.float64))
+        if F.ndim != 2 or F.shape[1] != ndof:
+            raise ValueError(f"F must have {ndof} entries per load case")
+
+    # ---- masks (optimizer.py:346-405) ----
+    protected_zone_mask, obstacle_mask, free_mask = resolve_masks(
+        nelx, nely, nelz, obstacle_mask, protected_zone_mask, force_field, support_mask, F)
+    design_nele = int(np.sum(free_mask))
+    target_free_volume = float(volfrac * design_nele)
 
     # ---- setup (optimizer.py:427-463) on the device ----
-    if F is None:
-        Fh = build_force_vector(nelx, nely, nelz, ndof, force_field)[None, :]
-    else:
-        Fh = np.atleast_2d(np.asarray(F, dtype=np.float64))
-        if Fh.shape[1] != ndof:
-            raise ValueError(f"F must have {ndof} entries per load case")
+    Fh = build_force_vector(nelx, nely, nelz, ndof, force_field)[None, :] if F is None else F
     KE = _ke(material_params, elem_size)
     H, Hs = build_filter(nelx, nely, nelz, rmin)
     solid, void, free = (to_flat_mask(protected_zone_mask), to_flat_mask(obstacle_mask),
@@ -392,7 +421,7 @@ def top3d(
             if record is not None:
                 record.append(dict(beta=beta, c=c, change=change, cg_iterations=cg_iters,
                                    relres=solver.last_relres, bisection_steps=int(host[3]),
-                                   lam=float(host[1])))
+                                   lam=float(host[1]), x=x.clone()))
             if save_history and ((total_loop - 1) % history_frequency == 0 or change <= tolx
                                  or stage_loop == maxloop):
                 history["density_history"].append(snap.numpy().reshape(nelz, nelx, nely).transpose(2, 1, 0).copy())

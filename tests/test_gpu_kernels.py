@@ -248,3 +248,72 @@ def test_oc_bisection_path_matches_reference(P, golden, tag, max_iter, tol):
                         target, beta, eta, xn, rn, OCWorkspace(H), max_iter, tol).cpu().numpy()
     assert int(st[2]) == steps
     assert st[0] == best and st[5] == lo and st[6] == hi
+
+
+@pytest.mark.parametrize("max_iter", [39, 40, 80])
+def test_oc_bisection_ties_keep_the_first_step(P, max_iter):
+    """A volume plateau: every free design value is 0.5 and the move limit 0.2,
+    so for every multiplier above about 2.8 each candidate sits at its lower
+    move limit and the projected volume is the same.  With the target just
+    above that volume, the reference's first 38 midpoints tie, and it keeps the
+    FIRST of them (strict <, oc_update.py:106); the reported multiplier must be
+    that one, with the same steps and final bracket."""
+    from pytopo3d_b200.oc_update import OCWorkspace, oc_update_flat
+    from pytopo3d_b200._tensors import to_flat, to_flat_mask, vec
+
+    nx, ny, nz, rmin, beta, eta, move = 8, 5, 4, 2.0, 2.0, 0.5, 0.2
+    shape = (ny, nx, nz)
+    rng = np.random.default_rng(21)
+    solid = np.zeros(shape, bool)
+    solid[:, 0, :] = True
+    void = np.zeros(shape, bool)
+    void[2, 4, 1:3] = True
+    free = ~(solid | void)
+    x = np.full(shape, 0.5)
+    x[solid], x[void] = 1.0, 0.0
+    Ho, Hso = O.build_filter(nx, ny, nz, rmin)
+    _, _, dp = O.build_physical_density(x, Ho, Hso, beta, eta, solid, void)
+    dc = O.apply_density_filter_chain_rule(-np.abs(rng.normal(size=shape)), dp, Ho, Hso)
+    dv = O.apply_density_filter_chain_rule(free.astype(float), dp, Ho, Hso)
+    low = x.copy()
+    low[free] = x[free] - move
+    _, rho_low, _ = O.build_physical_density(low, Ho, Hso, beta, eta, solid, void)
+    target = float(rho_low[free].sum()) + 1e-6
+    steps, best, lo, hi = _oracle_bisection((x, dc, dv, move, target, Ho, Hso, beta, eta, free, solid, void),
+                                            max_iter, 1e-8)
+    H, Hs = P.build_filter(nx, ny, nz, rmin)
+    xf = to_flat(x)
+    xn, rn = torch.empty_like(xf), torch.empty_like(xf)
+    st = oc_update_flat(H, xf, to_flat(dc), to_flat(dv), vec(Hs), to_flat_mask(solid), to_flat_mask(void), move,
+                        target, beta, eta, xn, rn, OCWorkspace(H), max_iter, 1e-8).cpu().numpy()
+    if max_iter == 39:
+        assert best == 5.0e11  # the tie is real: the reference keeps step 1
+    assert int(st[2]) == steps
+    assert st[0] == best and st[5] == lo and st[6] == hi
+
+
+def test_expired_barrier_wait_reaches_the_host(P, golden):
+    """Every grid-barrier wait of the OC kernel is bounded.  The wait-expiry hook
+    makes the barrier wait for a block that never arrives, with a short poll
+    limit: the launch must end by itself, the drop-in must raise Topo3dError,
+    and the context must stay usable (the same update then completes and
+    matches the reference)."""
+    from pytopo3d_b200 import _lib
+
+    L = _lib.lib()
+    nx, ny, nz, r = golden["oc_dims"]
+    H, Hs = P.build_filter(int(nx), int(ny), int(nz), float(r))
+    solid, void = golden["oc_solid"], golden["oc_void"]
+    free = ~(solid | void)
+    args = (golden["oc_x"], golden["oc_dc_dx"], golden["oc_dv_dx"], 0.2, float(golden["oc_target"]), H, Hs, 2.0,
+            0.5, free, solid, void)
+    assert L.tp3d_debug_expire_oc_waits(4096, 1) == 0
+    try:
+        with pytest.raises(_lib.Topo3dError, match="bounded device wait"):
+            P.optimality_criteria_update_projected(*args)
+    finally:
+        assert L.tp3d_debug_expire_oc_waits(0, 0) == 0
+    torch.cuda.synchronize()
+    bx, brho = P.optimality_criteria_update_projected(*args)
+    np.testing.assert_allclose(bx, golden["oc_best_x"], rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(brho, golden["oc_best_rho"], rtol=1e-12, atol=1e-13)

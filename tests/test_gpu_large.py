@@ -45,3 +45,28 @@ def test_large_cantilever_runs_and_meets_the_volume_target():
     assert abs(c_m - c_r) <= 1e-6 * abs(c_r)
     ref.close()
     loop.close()
+
+
+def test_config2_mixed_solve_within_1e6_of_fp64():
+    """The 128x64x64 cantilever (void cylinder r 12 along y, solid slab x < 4,
+    beta 1): after five loop iterations in the mixed form, one mixed solve of the
+    current design and warm start against an FP64 solve of the same system to a
+    relative residual of 1e-12.  The compliance (u'Ku, FP64 operator) must agree
+    within 1e-6; the displacement error (relative 2-norm) is reported and bounded
+    at 1e-5."""
+    import bench
+    from pytopo3d_b200.optimizer import SimpLoop
+    from pytopo3d_b200.stiffness import lk_H8
+
+    shape, solid, void, F, fixed = bench.workload(128, 64, 64)
+    loop = SimpLoop(128, 64, 64, 0.3, 3.0, 3.0, lk_H8(elem_size=1.0), F, fixed, solid, void, precision="mixed")
+    loop.set_beta(1.0)
+    for _ in range(5):
+        loop.step()
+    acc = bench.accuracy_vs_fp64(loop, "mixed")
+    print(f"128x64x64 mixed vs fp64: compliance {acc['compliance_rel_err']:.2e}, "
+          f"displacement {acc['displacement_rel_err']:.2e}, fp64 relres {acc['reference']['relres']:.1e}")
+    assert acc["reference"]["relres"] <= 1e-11
+    assert acc["compliance_rel_err"] <= 1e-6
+    assert acc["displacement_rel_err"] <= 1e-5
+    loop.close()

@@ -5,7 +5,7 @@ import pytest
 
 import pytopo3d_b200 as P
 from pytopo3d_b200.assembly import grid_from_edof
-from pytopo3d_b200.obstacles import create_cylinder_obstacle
+from pytopo3d_b200.obstacles import CUBE, SPHERE, cylinder_params
 
 ORTHO = (10.0, 20.0, 30.0, 4.0, 5.0, 6.0, 0.10, 0.12, 0.08)
 
@@ -55,11 +55,29 @@ def test_out_of_range_boxes_raise():
         P.build_supports(3, 2, 4, 180, np.zeros((1, 1, 1), bool))
 
 
-def test_cylinder_masks_match_reference(golden):
-    np.testing.assert_array_equal(create_cylinder_obstacle((16, 32, 16), (0.5, 0.5, 0.5), 0.25, 1.0, 1),
-                                  golden["cyl_y"])
-    np.testing.assert_array_equal(create_cylinder_obstacle((10, 12, 14), (0.3, 0.6, 0.5), 0.3, 0.5, 0),
-                                  golden["cyl_x"])
+def primitive_mask(shape, o):
+    """Test-side evaluation of one tp3d_obstacle's integer parameters, element by
+    element, as the mask kernel's inside() does."""
+    nely, nelx, nelz = shape
+    yy, xx, zz = np.ogrid[:nely, :nelx, :nelz]
+    c = [xx, yy, zz]
+    if o.kind == CUBE:
+        m = np.ones(shape, bool)
+        for k in range(3):
+            m &= (c[k] >= o.lo[k]) & (c[k] < o.hi[k])
+        return m
+    d2 = sum((c[k] - o.center[k]) ** 2 for k in range(3) if o.kind == SPHERE or k != o.axis)
+    m = d2 <= o.r2
+    if o.kind != SPHERE:
+        m = m & (c[o.axis] >= o.lo[o.axis]) & (c[o.axis] < o.hi[o.axis])
+    return np.broadcast_to(m, shape)
+
+
+def test_cylinder_parameters_reproduce_reference_masks(golden):
+    # the integer parameters the mask kernel receives (obstacles.py:137-160)
+    for shape, args, key in (((16, 32, 16), ((0.5, 0.5, 0.5), 0.25, 1.0, 1), "cyl_y"),
+                             ((10, 12, 14), ((0.3, 0.6, 0.5), 0.3, 0.5, 0), "cyl_x")):
+        np.testing.assert_array_equal(primitive_mask(shape, cylinder_params(shape, *args)), golden[key])
 
 
 def test_top3d_validation_happens_before_any_device_work():

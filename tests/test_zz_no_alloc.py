@@ -4,11 +4,14 @@ Some callers cannot allocate device memory per call: applications whose device
 memory is reserved up front by their own allocator, or code that cannot accept
 the implicit device synchronisation of cudaMalloc / cudaFree.  For them the
 library offers an OC update whose scratch is a static device array.  These
-tests call it through the C ABI, twice in a row on different designs, and
-compare it with the allocating entry point ``tp3d_oc_update`` at the tolerance
-of the other OC tests (1e-12).  This file is collected last so that a run that
-stops at the first failure has already run every other test; it also passes
-on its own in a fresh process (the first call does the per-device set-up).
+tests call it through the C ABI, three times in a row on different designs
+(a small grid, a filter radius at the stencil's limit, and a grid of exactly
+the static maximum of elements), and compare it with the allocating entry
+point ``tp3d_oc_update``: both run the same kernel on the same launch grid,
+so the results must agree bit for bit.  This file is collected last so that a
+run that stops at the first failure has already run every other test; it also
+passes on its own in a fresh process (the first call does the per-device
+set-up).
 """
 
 import numpy as np
@@ -19,16 +22,20 @@ from oracle import simp_oracle as O
 
 
 def _problem(nx, ny, nz, rmin, seed):
+    """A seeded OC input: design, filtered sensitivities of the cantilever masks."""
+    import pytopo3d_b200 as P
+
     rng = np.random.default_rng(seed)
     shape = (ny, nx, nz)
     solid, void, free = O.prepare_masks(nx, ny, nz)
     x = rng.uniform(0.1, 0.9, size=shape)
     x[solid], x[void] = 1.0, 0.0
-    H, Hs = O.build_filter(nx, ny, nz, rmin)
-    _, _, dp = O.build_physical_density(x, H, Hs, 2.0, 0.5, solid, void)
+    H, Hs = P.build_filter(nx, ny, nz, rmin)
+    _, _, dp = P.build_physical_density(x, H, Hs, 2.0, 0.5, solid, void)
     dc = -np.abs(rng.normal(size=shape))
-    dc_dx = O.apply_density_filter_chain_rule(dc, dp, H, Hs)
-    dv_dx = O.apply_density_filter_chain_rule(free.astype(float), dp, H, Hs)
+    dc_dx = P.apply_density_filter_chain_rule(dc, dp, H, Hs)
+    dv_dx = P.apply_density_filter_chain_rule(free.astype(float), dp, H, Hs)
+    Hs = Hs.cpu().numpy() if isinstance(Hs, torch.Tensor) else np.asarray(Hs)
     return x, dc_dx, dv_dx, Hs, solid, void, 0.3 * int(free.sum())
 
 
@@ -62,16 +69,19 @@ def test_noalloc_oc_update_matches_allocating_entry_point():
     from pytopo3d_b200 import _lib
 
     L = _lib.lib()
-    cases = [((16, 8, 8), 2.5, 1), ((23, 9, 7), 1.5, 2)]  # two calls in a row, different sizes / radii
+    cap = L.tp3d_oc_noalloc_max_elements()
+    # calls in a row on different sizes and radii: rmin 6.9 fills the largest
+    # column table (offsets up to 6), 64x64x64 is exactly the element limit
+    cases = [((16, 8, 8), 2.5, 1), ((23, 9, 7), 6.9, 2), ((64, 64, 64), 1.5, 3)]
+    assert 64 * 64 * 64 == cap
     for dims, rmin, seed in cases:
         args = _problem(*dims, rmin, seed)
         nbytes = L.tp3d_oc_scratch_bytes(*dims, rmin)
         scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
         ref = _run(L, L.tp3d_oc_update, dims, rmin, args, scratch)
         got = _run(L, L.tp3d_oc_update_noalloc, dims, rmin, args)
-        for a, b in zip(got[:2], ref[:2]):
-            np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-13)
-        np.testing.assert_allclose(got[2], ref[2], rtol=1e-12, atol=1e-13)
+        for a, b in zip(got, ref):
+            np.testing.assert_array_equal(a, b)
         assert np.isfinite(got[2][2]) and got[2][2] >= 1  # bisection steps recorded
 
 
