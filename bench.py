@@ -133,15 +133,58 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_loop(precision, x0=None, solver_options=None):
+def make_loop(precision, x0=None, solver_options=None, dims=None, volfrac=VOLFRAC, rmin=RMIN, masks=True):
+    """The cantilever loop at `dims` (default: the 128x64x64 workload).  masks=False:
+    the plain cantilever (default load strip and support face only, no cylinder or
+    slab), the configuration the reference's own CPU path runs at 32x16x16."""
     from pytopo3d_b200.optimizer import SimpLoop
     from pytopo3d_b200.stiffness import lk_H8
 
-    shape, solid, void, F, fixed = workload(NELX, NELY, NELZ)
-    loop = SimpLoop(NELX, NELY, NELZ, VOLFRAC, PENAL, RMIN, lk_H8(elem_size=1.0), F, fixed, solid, void,
+    nelx, nely, nelz = dims or (NELX, NELY, NELZ)
+    shape, solid, void, F, fixed = workload(nelx, nely, nelz) if masks else plain_cantilever(nelx, nely, nelz)
+    loop = SimpLoop(nelx, nely, nelz, volfrac, PENAL, rmin, lk_H8(elem_size=1.0), F, fixed, solid, void,
                     projection_eta=ETA, move=MOVE, precision=precision, x0=x0, solver_options=solver_options)
     loop.set_beta(BETA)
     return loop
+
+
+def plain_cantilever(nelx, nely, nelz):
+    """The reference's default cantilever: load strip and support face protected
+    (optimizer.py:366-390), no obstacles, total unit -z load on the x = nelx, z = 0 edge."""
+    from pytopo3d_b200.assembly import build_force_vector, build_supports
+
+    shape = (nely, nelx, nelz)
+    solid = np.zeros(shape, bool)
+    solid[:, -1, 0] = True
+    solid[:, 0, :] = True
+    void = np.zeros(shape, bool)
+    ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
+    F = build_force_vector(nelx, nely, nelz, ndof) / (nely + 1)
+    free, _ = build_supports(nelx, nely, nelz, ndof)
+    fixed = np.ones(ndof, np.uint8)
+    fixed[free] = 0
+    return shape, solid, void, F, fixed
+
+
+def e2e_rate_of(loop_factory, warm, steps, dist, world):
+    """SIMP it/s through SimpLoop.step_host (pinned H2D of the design, D2H of the
+    new design and the compliance every step), wall clock around `steps` steps
+    after `warm` steps, max over ranks."""
+    import torch
+
+    loop = loop_factory()
+    x_host = loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
+    for _ in range(warm):
+        x_host, _ = loop.step_host(x_host)
+    barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        x_host, _ = loop.step_host(x_host)
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, dist)
+    loop.close()
+    return job_rate(steps, dt, world)
 
 
 def time_device_steps(loop, steps, dist):
@@ -249,9 +292,8 @@ def run_reference(args, rank):
     if rank != 0:
         return 0
     steps = max(1, args.steps)
-    warm = min(1, args.warmup)
-    if warm:
-        cpu_reference_sample(1)
+    warm = max(3, args.warmup)  # the same warm-up rule as the B200 arm
+    cpu_reference_sample(warm)
     rate, dt = cpu_reference_sample(steps)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     line = {
@@ -259,7 +301,8 @@ def run_reference(args, rank):
         "steps": steps, "warmup": warm, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "cantilever 32x16x16 (reference CPU path: SuperLU spsolve); the 128x64x64 "
-                               "workload does not fit the reference's direct solve", "beta": BETA,
+                               "workload does not fit the reference's direct solve; the B200 line's "
+                               "same_config_as_reference object times this same workload", "beta": BETA,
                    "rmin": RMIN, "volfrac": VOLFRAC},
         "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": 1, "kind": "port",
                          "sample": f"{steps} loop bodies of the oracle restatement at 32x16x16 "
@@ -278,6 +321,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-large", action="store_true", help="skip the 256x128x128 design")
     ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply", "batch"],
                     help="step: warm-up + --steps loop bodies only (for launch lists); "
                          "apply: fine-operator launches only (for kernel captures)")
@@ -316,25 +360,21 @@ def main():
     W = max(3, args.warmup)
     results = {}
     for prec in ([args.precision] + [p for p in ("fp64", "mixed") if p != args.precision]):
+        # both precisions: the same warm-up, the same number of timed steps
         loop = make_loop(prec)
-        if prec == args.precision:
-            with ClockSampler(local) as clk:
-                for _ in range(W):
-                    loop.step()
-                torch.cuda.synchronize()
-                with clk.timed():
-                    ms, cg, launches, c = time_device_steps(loop, args.steps, dist)
-            clocks = clk.summary()
-        else:
+        with ClockSampler(local) as clk:
             for _ in range(W):
                 loop.step()
             torch.cuda.synchronize()
-            ms, cg, launches, c = time_device_steps(loop, max(3, args.steps // 4), dist)
-        steps = args.steps if prec == args.precision else max(3, args.steps // 4)
+            with clk.timed():
+                ms, cg, launches, c = time_device_steps(loop, args.steps, dist)
+        if prec == args.precision:
+            clocks = clk.summary()
+        steps = args.steps
         ms = max_over_ranks(ms, dist)
         apply_ms = (ctypes_time_apply(loop.solver, fp32=(prec == "mixed")))
         results[prec] = dict(ms=ms, steps=steps, cg=cg, launches=launches, c=c, apply_ms=apply_ms,
-                             loop=loop, stats=loop.solver.stats())
+                             loop=loop, stats=loop.solver.stats(), clocks=clk.summary())
         results[prec]["accuracy"] = accuracy_vs_fp64(loop, prec)
         if prec != args.precision:
             loop.close()
@@ -349,20 +389,23 @@ def main():
     # end-to-end through the public API with host buffers (pinned H2D of x, D2H of x_new + c):
     # a fresh loop from the same start, the same warm-up and the same number of
     # steps as the device-timed run, so both follow the same trajectory
-    e2e_loop = make_loop(args.precision)
-    x_host = e2e_loop.design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
-    for _ in range(W):
-        x_host, _ = e2e_loop.step_host(x_host)
-    barrier(dist)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e_steps = steps
-    for _ in range(e_steps):
-        x_host, c_host = e2e_loop.step_host(x_host)
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e_rate = job_rate(e_steps, e2e_s, world)
-    e2e_loop.close()
+    e2e_rate = e2e_rate_of(lambda: make_loop(args.precision), W, steps, dist, world)
+
+    # the reference's own CPU workload (the plain 32x16x16 cantilever, which its
+    # direct solve can run) on the B200, both precisions, same warm-up and steps:
+    # the like-for-like partner of the --impl reference line
+    same = {"workload": "cantilever 32x16x16, no obstacles, beta 1 (the --impl reference workload)"}
+    for prec in ("fp64", "mixed"):
+        mk = lambda: make_loop(prec, dims=(32, 16, 16), masks=False)
+        sl = mk()
+        for _ in range(W):
+            sl.step()
+        torch.cuda.synchronize()
+        sms, scg, _, _ = time_device_steps(sl, args.steps, dist)
+        sl.close()
+        same[prec] = {"value": job_rate(args.steps, max_over_ranks(sms, dist) / 1e3, world), "unit": "iter/s",
+                      "cg_iterations_per_step": scg / args.steps,
+                      "e2e": e2e_rate_of(mk, W, args.steps, dist, world)}
 
     # roofline of the dominant kernel (fine-level operator apply)
     peak, peak_kind = peaks()
@@ -372,9 +415,13 @@ def main():
     bf16 = bool(getattr(loop.solver.opts, "inner_density", 0))
     alg_bytes = (8 * ndof + (2 if bf16 else 4) * nele) if fp32 else (16 * ndof + 8 * nele)
     achieved = alg_bytes / (main_r["apply_ms"] * 1e-3) / 1e9
-    flops = 1152.0 * (NELX + 1) * (NELY + 1) * (NELZ + 1)
+    nnode = (NELX + 1) * (NELY + 1) * (NELZ + 1)
     form = main_r["stats"].get("fine_form_fp32" if fp32 else "fine_form_fp64", 0)
     kname = "wht_apply" if form and form >= 1 else "fine_apply"
+    # floating-point operations the kernel executes per node (FMA = 2): the
+    # Walsh-Hadamard block form does 99 FMAs and 81 adds per node and plane; the
+    # dense-KE form the dense 576 FMAs per element
+    flops_node = 279.0 if kname == "wht_apply" else 1152.0
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -382,6 +429,34 @@ def main():
             traffic = json.load(open(tf)).get(kname + ("_f32" if fp32 else "_f64"))
         except Exception:
             traffic = None
+    # the largest coarse-level kernel (level 1, packed stencil), cold L2
+    c_ms, c_bytes = loop.solver.time_level(1, fp32, 10)
+    c_gbs = c_bytes / (c_ms * 1e-3) / 1e9
+    # step level: the CG loop's algorithmic bytes (summed over the kernels of one
+    # captured iteration) times the iterations per step, over the whole step time
+    bpi = main_r["stats"].get("bytes_per_cg_iteration", 0.0)
+    step_gbs = bpi * (main_r["cg"] / steps) / (main_r["ms"] / steps * 1e-3) / 1e9
+
+    # the large single design (256x128x128, volfrac 0.2, rmin 4.5, beta 1, mixed):
+    # a short device-timed run of the same loop body
+    large = None
+    if not args.no_large:
+        ll = make_loop("mixed", dims=(256, 128, 128), volfrac=0.2, rmin=4.5)
+        for _ in range(W):
+            ll.step()
+        torch.cuda.synchronize()
+        lsteps = max(3, args.steps // 2)
+        lms, lcg, _, _ = time_device_steps(ll, lsteps, dist)
+        lms = max_over_ranks(lms, dist)
+        l_ndof = 3 * 257 * 129 * 129
+        l_apply = ctypes_time_apply(ll.solver, fp32=True)
+        l_bytes = 8 * l_ndof + 4 * 256 * 128 * 128
+        large = {"workload": "cantilever 256x128x128, volfrac 0.2, rmin 4.5, beta 1, mixed", "steps": lsteps,
+                 "warmup": W, "value": job_rate(lsteps, lms / 1e3, world), "unit": "iter/s",
+                 "dof_cg_iters_per_s": world * l_ndof * lcg / (lms / 1e3), "cg_iterations_per_step": lcg / lsteps,
+                 "fine_operator": {"launch_ms": l_apply, "bytes_per_launch": l_bytes,
+                                   "achieved": l_bytes / (l_apply * 1e-3) / 1e9, "frac": l_bytes / (l_apply * 1e-3) / 1e9 / peak}}
+        ll.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -408,15 +483,30 @@ def main():
         "other_precision": {p: {"value": world * results[p]["steps"] / (results[p]["ms"] / 1e3),
                                 "ms_per_step": results[p]["ms"] / results[p]["steps"],
                                 "cg_iterations_per_step": results[p]["cg"] / results[p]["steps"],
-                                "apply_ms": results[p]["apply_ms"], "accuracy_vs_fp64": results[p]["accuracy"]}
+                                "apply_ms": results[p]["apply_ms"], "accuracy_vs_fp64": results[p]["accuracy"],
+                                "steps": results[p]["steps"], "warmup": W,
+                                "bytes_per_cg_iteration": results[p]["stats"].get("bytes_per_cg_iteration"),
+                                "kernels_per_cg_iteration": results[p]["stats"].get("kernels_per_cg_iteration"),
+                                "clocks": results[p]["clocks"]}
                             for p in other},
         "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": 8 * nele,
                 "d2h_bytes_per_step": 8 * nele + 8},
+        "same_config_as_reference": same,
         "roofline": {"bound": "hbm", "kernel": kname + "_kernel<" + ("float" if fp32 else "double") + ">",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic, "bytes_per_launch": alg_bytes,
                      "launch_ms": main_r["apply_ms"],
-                     "flop_rate_tflops": flops / (main_r["apply_ms"] * 1e-3) / 1e12},
+                     "executed_flops_per_node": flops_node,
+                     "executed_tflops": flops_node * nnode / (main_r["apply_ms"] * 1e-3) / 1e12},
+        "roofline_coarse": {"bound": "hbm", "kernel": "stencil_apply_kernel (level 1, packed "
+                                                      + ("bf16" if fp32 else "fp64") + " stencil, cold L2)",
+                            "achieved": c_gbs, "peak": peak, "unit": "GB/s", "frac": c_gbs / peak,
+                            "bytes_per_launch": c_bytes, "launch_ms": c_ms},
+        "roofline_step": {"bound": "hbm", "what": "algorithmic bytes of the CG loop's kernels per step / step time",
+                          "bytes_per_cg_iteration": bpi,
+                          "kernels_per_cg_iteration": main_r["stats"].get("kernels_per_cg_iteration"),
+                          "achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak},
+        "large_design": large,
         "cpu_baseline": cpu,
         "gpu_launches": main_r["launches"],
         "clocks": clocks,

@@ -294,6 +294,15 @@ int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
  * counterpart. */
 int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch);
 
+/* Average device time (ms) of one Apply-mode launch of the level-`level` operator (0: the fine
+ * operator; >= 1: the coarse packed-stencil kernel of the V-cycle; the coarsest dense level is
+ * excluded), each launch timed alone with its own CUDA events after a 256 MiB write that evicts
+ * L2, so it reads its operator and vectors from HBM; *bytes_per_launch receives its algorithmic
+ * bytes (vectors in and out, stencil or moduli, fixed-DOF mask).  fp32 != 0: the mixed form's
+ * kernels.  Measurement helper for the roofline figures; no reference counterpart. */
+int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int launches, double* ms_per_launch,
+                           double* bytes_per_launch);
+
 /* Diagnostics of the last solve, in this order: levels, CG iterations, reliable updates
  * (mixed), relres, restarts (FP64), coarsest dense size, dense-form tile (y, x, z chunk),
  * coarsest-inverse fallback flag, lambda_max(Dinv A) of the fine level, residual-floor flag,
@@ -303,7 +312,10 @@ int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_pe
  * solve) rather than host-polled, the programmatic-dependent-launch mask in use (0 none),
  * the number of levels whose stencils are held in bf16, the coarsest inverse's status (0 first
  * attempt, 1-3 attempts with a raised diagonal, 4 diagonal fallback), the level run as one block
- * with the coarsest solve (0 none).  Returns the count written. */
+ * with the coarsest solve (0 none), the algorithmic bytes of one CG iteration (every array each
+ * kernel of the iteration must read or write once, summed over the iteration's kernels; the
+ * reliable-update branch excluded; 0 before the first solve), the kernels launched per CG
+ * iteration.  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

@@ -34,10 +34,31 @@ namespace tp3d {
 namespace {
 // While a graph is being captured launches are counted into the graph's tally.
 thread_local long long* t_capture_count = nullptr;
+// ... and, for the CG iteration graph, each launch's algorithmic bytes (the
+// arrays it must read and write once; the measure of the step-level roofline).
+thread_local double* t_capture_bytes = nullptr;
 }  // namespace
 inline void count_launch() {
   if (t_capture_count) ++*t_capture_count;
   else add_launches(1);
+}
+inline void count_bytes(double b) {
+  if (t_capture_bytes) *t_capture_bytes += b;
+}
+
+// Algorithmic bytes of one operator launch in mode MODE over a level with n
+// DOFs and nn nodes: input and output vectors, `src` bytes of moduli or
+// stencil, the fixed-DOF mask (a byte per node), and the mode's epilogue
+// vectors (right-hand side, inverse diagonal, Chebyshev direction read/written).
+template <typename T, int MODE>
+double op_bytes(long long n, long long nn, double src) {
+  const double w = (double)sizeof(T);
+  double b = 2.0 * w * n + src + (double)nn;
+  if (epi_reads_b<MODE>()) b += w * n;
+  if (epi_reads_dinv<MODE>()) b += w * n;
+  if (MODE == kModeChebStep || MODE == kModeChebStepDot) b += w * n;
+  if (MODE == kModeChebFirst || MODE == kModeChebStep || MODE == kModeChebStepDot) b += w * n;
+  return b;
 }
 
 constexpr int kMaxPartials = 1 << 16;
@@ -59,6 +80,7 @@ struct KrylovVec {
   T *u = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
   cudaGraphExec_t graph = nullptr;
   long long graph_kernels = 0;
+  double graph_bytes = 0.0;  // algorithmic bytes of one CG iteration (reliable-update branch excluded)
   // device-side loop (conditional nodes): kernels per pass, and in the
   // reliable-update branch
   bool loop = false;
@@ -321,8 +343,15 @@ struct tp3d_solver {
   }
 
   // ---------------- operators ----------------
+  // bytes per element of the fine operator's modulus source
+  template <typename T>
+  double fine_src_bytes() const {
+    if constexpr (sizeof(T) == 8) return 8.0;
+    else return rho16 ? 2.0 : 4.0;
+  }
   template <typename T, int MODE>
   int fine(const OpIO<T>& io) {
+    count_bytes(op_bytes<T, MODE>(3 * g.nnode(), g.nnode(), fine_src_bytes<T>() * (double)g.nele()));
     if (use_wht<T>()) return fine_wht<T>(MODE, io);
     const dim3 grid(tile.tiles_y * tile.tiles_x, tile.zchunks);
     int rc;
@@ -468,6 +497,52 @@ struct tp3d_solver {
     return rc;
   }
 
+  // Average device time of `launches` Apply-mode launches of the level-L
+  // operator (L >= 1: the packed-stencil kernel of the V-cycle; L = 0: the fine
+  // operator), each timed alone with its own event pair after a 256 MiB memset
+  // that evicts L2, so every launch reads its stencil and vectors from HBM.
+  // *bytes_out: the launch's algorithmic bytes (op_bytes).
+  template <typename T>
+  int time_level_cold(int L, int launches, double* ms_out, double* bytes_out) {
+    constexpr size_t kFlushBytes = (size_t)256 << 20;
+    auto& lv = levels<T>()[L];
+    if (!lv.x[0] || !lv.x[1]) return TP3D_ERR_ARG;
+    const long long nn = grids[L].nnode(), n = 3 * nn;
+    const double src = L == 0 ? fine_src_bytes<T>() * (double)g.nele() : 81.0 * stencil_bytes<T>(L) * (double)n;
+    *bytes_out = op_bytes<T, kModeApply>(n, nn, src);
+    unsigned char* flush = nullptr;
+    if (cudaMalloc(&flush, kFlushBytes) != cudaSuccess) {
+      tp3d_set_last_error("timing buffers: allocation failed");
+      return TP3D_ERR_CUDA;
+    }
+    struct Free {
+      unsigned char* p;
+      ~Free() { cudaFree(p); }
+    } guard{flush};
+    cudaEvent_t a, b;
+    TP3D_CHECK(cudaEventCreate(&a));
+    TP3D_CHECK(cudaEventCreate(&b));
+    OpIO<T> io;
+    io.u = lv.x[0];
+    io.out = lv.x[1];
+    int rc = apply_level<T, kModeApply>(L, io);  // warm-up (instruction cache, first-launch costs)
+    double total = 0.0;
+    for (int k = 0; k < launches && rc == TP3D_OK; ++k) {
+      if (cudaMemsetAsync(flush, k & 0xff, kFlushBytes, st) != cudaSuccess) rc = TP3D_ERR_CUDA;
+      if (rc == TP3D_OK && cudaEventRecord(a, st) != cudaSuccess) rc = TP3D_ERR_CUDA;
+      if (rc == TP3D_OK) rc = apply_level<T, kModeApply>(L, io);
+      if (rc == TP3D_OK && cudaEventRecord(b, st) != cudaSuccess) rc = TP3D_ERR_CUDA;
+      float ms = 0.f;
+      if (rc == TP3D_OK && (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess))
+        rc = TP3D_ERR_CUDA;
+      total += ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms_out = total / launches;
+    return rc;
+  }
+
   // Fine operator form for precision T: the dense-KE kernel or one of the
   // Walsh-Hadamard variants, whichever runs the Apply mode fastest on this
   // grid with cold inputs (time_fine_cold, 12 launches each);
@@ -517,6 +592,7 @@ struct tp3d_solver {
     if (L == 0) return fine<T, MODE>(io);
     const long long ndof = 3 * grids[L].nnode();
     const bool split = ndof <= o.split_dofs;  // four lanes per DOF on the small levels
+    count_bytes(op_bytes<T, MODE>(ndof, grids[L].nnode(), 81.0 * stencil_bytes<T>(L) * (double)ndof));
     if constexpr (sizeof(T) == 4) {
       if (L < (int)S16.size() && S16[L]) {
         StencilParams<float, __nv_bfloat16> p;
@@ -543,6 +619,14 @@ struct tp3d_solver {
     else launch(kPdlCoarse, stencil_apply_kernel<T, MODE>, dim3(grid_blocks(ndof)), dim3(256), 0, p);
     TP3D_CHECK_LAUNCH();
     return TP3D_OK;
+  }
+
+  // bytes per stencil coefficient of level L >= 1 in precision T's cycle
+  template <typename T>
+  double stencil_bytes(int L) const {
+    if constexpr (sizeof(T) == 4)
+      if (L < (int)S16.size() && S16[L]) return 2.0;
+    return (double)sizeof(T);
   }
 
   // ---------------- V-cycle ----------------
@@ -623,6 +707,10 @@ struct tp3d_solver {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    for (int k = L; k < nlev; ++k) {
+      const double n = 3.0 * grids[k].nnode();
+      count_bytes(81.0 * stencil_bytes<T>(k) * n + 5.0 * sizeof(T) * n);
+    }
     if (cudaLaunchKernelEx(&cfg, coarse_cycle_kernel<T>, p) != cudaSuccess) *rc = TP3D_ERR_CUDA;
     count_launch();
     return L == nlev - 1 ? lvs[L].x[0] : lvs[L].x[cycle_final_buffer(pre_sweeps(L), post_sweeps(L))];
@@ -693,6 +781,11 @@ struct tp3d_solver {
       p.omega = (float)o.omega;
       p.done = done;
     };
+    {
+      const double n = 3.0 * grids[L].nnode();
+      count_bytes(81.0 * stencil_bytes<float>(L) * n + 4.0 * cn * cn + 4.0 * sizeof(float) * n +
+                  (double)grids[L].nnode());
+    }
     if (S16[L]) {
       DeepParams<float, __nv_bfloat16> p;
       fill(p);
@@ -722,6 +815,7 @@ struct tp3d_solver {
     const Grid& gl = grids[L];
     const long long ndof = 3 * gl.nnode();
     if (nlev == 1) {  // no hierarchy: Jacobi preconditioner
+      count_bytes(3.0 * sizeof(T) * ndof);
       launch(kPdlFine, smooth_zero_kernel<T>, dim3(grid_blocks(ndof)), dim3(256), 0, ndof, b, (const T*)lv.dinv, T(1),
              (const double*)nullptr, lv.x[0], (T*)nullptr, done);
       return lv.x[0];
@@ -730,6 +824,7 @@ struct tp3d_solver {
       const T* inv;
       if constexpr (sizeof(T) == 8) inv = cinv64;
       else inv = cinv32;
+      count_bytes((double)sizeof(T) * cn * cn + 2.0 * sizeof(T) * cn);
       launch(kPdlCoarse, dense_matvec_kernel<T>, dim3(std::max(1, std::min(cn / 8 + 1, nsm))), dim3(256), 0, cn, inv,
              b, lv.x[0], done);
       return lv.x[0];
@@ -740,6 +835,7 @@ struct tp3d_solver {
     const bool cheb = o.smoother != 1;
     int cur = 0;
     if (!zero_done) {
+      count_bytes((cheb ? 4.0 : 3.0) * sizeof(T) * ndof);
       launch(L == 0 ? kPdlFine : kPdlCoarse, smooth_zero_kernel<T>, dim3(grid_blocks(ndof)), dim3(256), 0, ndof, b,
              (const T*)lv.dinv, (T)o.omega, (const double*)(cheb ? coef[L] : nullptr), lv.x[cur],
              cheb ? lv.d : (T*)nullptr, done);
@@ -775,6 +871,8 @@ struct tp3d_solver {
         p.io.b = b;
         p.io.done = done;
       };
+      count_bytes(2.0 * sizeof(T) * ndof + 81.0 * stencil_bytes<T>(L) * ndof + (double)gl.nnode() +
+                  (double)gn.nnode() + (fuse_first ? 4.0 : 1.0) * sizeof(T) * 3.0 * gn.nnode());
       const dim3 grid((unsigned)gn.nnode());
       bool done16 = false;
       if constexpr (sizeof(T) == 4) {
@@ -795,10 +893,13 @@ struct tp3d_solver {
                (const uint8_t*)fix[L + 1], lc.b, fs);
       }
     } else {
+      count_bytes((double)sizeof(T) * ndof + (double)gn.nnode() +
+                  (fuse_first ? 4.0 : 1.0) * sizeof(T) * 3.0 * gn.nnode());
       launch(kPdlCoarse, restrict_kernel<T>, plane_grid((gn.nx + 1) * (gn.ny + 1), gn.nz + 1), dim3(256), 0, gl,
              gn, (const T*)lv.r, (const uint8_t*)fix[L + 1], lc.b, done, fs);
     }
     T* xc = vcycle<T>(L + 1, lc.b, done, rc, fuse_first);
+    count_bytes((double)sizeof(T) * 3.0 * gn.nnode() + 2.0 * sizeof(T) * ndof + (double)gl.nnode());
     launch(L == 0 ? kPdlFine : kPdlCoarse, prolong_add_kernel<T>, plane_grid((gl.nx + 1) * (gl.ny + 1), gl.nz + 1),
            dim3(256), 0, gl, gn, (const T*)xc, (const uint8_t*)fix[L], lv.x[cur], done);
     const bool dot_here = dot_op >= 0 && o.smoother != 1 && post_sweeps(L) >= 1;
@@ -815,12 +916,15 @@ struct tp3d_solver {
     cudaGraph_t gr = nullptr;
     TP3D_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     long long nk = 0;
+    double nbytes = 0.0;
     t_capture_count = &nk;
+    t_capture_bytes = &nbytes;
     pdl_region = true;
     plain_next = true;
     const int rc = body();
     pdl_region = false;
     t_capture_count = nullptr;
+    t_capture_bytes = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &gr);
     const cudaError_t e2 = (rc || e != cudaSuccess) ? cudaErrorUnknown : cudaGraphInstantiate(&K.graph, gr, 0);
     if (e == cudaSuccess && gr) cudaGraphDestroy(gr);
@@ -835,6 +939,7 @@ struct tp3d_solver {
       return TP3D_ERR_CUDA;
     }
     K.graph_kernels = nk;
+    K.graph_bytes = nbytes;
     return TP3D_OK;
   }
 
@@ -861,6 +966,7 @@ struct tp3d_solver {
     ok = ok && cudaGraphAddNode(&wnode, G, nullptr, 0, &cp) == cudaSuccess;
     bool capturing = false;
     long long nk = 0;
+    double nbytes = 0.0;
     int rc = TP3D_OK;
     if (ok) {
       cudaGraph_t B = cp.conditional.phGraph_out[0];
@@ -870,6 +976,7 @@ struct tp3d_solver {
     }
     if (ok) {
       t_capture_count = &nk;
+      t_capture_bytes = &nbytes;
       in_loop_capture = true;
       branch_count = 0;
       pdl_region = true;
@@ -880,6 +987,7 @@ struct tp3d_solver {
       ++nk;
       in_loop_capture = false;
       t_capture_count = nullptr;
+      t_capture_bytes = nullptr;
     }
     if (capturing) {
       cudaGraph_t out = nullptr;
@@ -901,6 +1009,7 @@ struct tp3d_solver {
     }
     K.loop = true;
     K.graph_kernels = nk;
+    K.graph_bytes = nbytes;
     K.branch_kernels = branch_count;
     return true;
   }
@@ -944,11 +1053,14 @@ struct tp3d_solver {
       rc = TP3D_ERR_CUDA;
     } else {
       long long* outer = t_capture_count;
+      double* outer_bytes = t_capture_bytes;
       long long nb = 0;
       t_capture_count = &nb;
+      t_capture_bytes = nullptr;  // the branch runs only on a reliable update
       plain_next = true;
       rc = branch();
       t_capture_count = outer;
+      t_capture_bytes = outer_bytes;
       cudaGraph_t out = nullptr;
       if (cudaStreamEndCapture(st, &out) != cudaSuccess) {
         branch_ok = false;
@@ -1046,14 +1158,17 @@ struct tp3d_solver {
     io.fin_count = fin_count;
     int rc = fine<double, kModeCgQ>(io);
     const CoarseFirstStep<double> fs0 = first_step<double>(0);
+    count_bytes((fs0.x0 ? 9.0 : 6.0) * 8.0 * ndof);
     launch(kPdlFine, cg_update_kernel<double>, dim3(nb), dim3(256), 0, ndof, K.u, (const double*)K.p, K.r,
            (const double*)K.q, state, partials, (int)kFinRR, fin_count, fs0);
     bool dot_done = false;
     double* z = vcycle<double>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZ, &dot_done);
     if (!dot_done) {
+      count_bytes(2.0 * 8.0 * ndof);
       launch(kPdlFine, dot_kernel<double>, dim3(nb), dim3(256), 0, ndof, (const double*)K.r, (const double*)z, partials,
              (const int*)done, (const int*)nullptr, state, (int)kFinRZ, fin_count);
     }
+    count_bytes(3.0 * 8.0 * ndof);
     launch(kPdlFine, cg_p_kernel<double>, dim3(nb), dim3(256), 0, ndof, (const double*)z, K.p,
            (const PcgState*)state, 0);
     TP3D_CHECK_LAUNCH();
@@ -1172,6 +1287,7 @@ struct tp3d_solver {
     io.fin_count = fin_count;
     int rc = fine<float, kModeCgQ>(io);
     const CoarseFirstStep<float> fs0 = first_step<float>(0);
+    count_bytes((fs0.x0 ? 9.0 : 6.0) * 4.0 * ndof);
     launch(kPdlFine, cg_update_kernel<float>, dim3(nb), dim3(256), 0, ndof, K.u, (const float*)K.p, K.r,
            (const float*)K.q, state, partials, (int)kFinRRMixed, fin_count, fs0);
     // reliable update (each kernel is also gated on state->update itself)
@@ -1198,9 +1314,11 @@ struct tp3d_solver {
     bool dot_done = false;
     float* z = vcycle<float>(0, K.r, done, &rc, fs0.x0 != nullptr, kFinRZMixed, &dot_done);
     if (!dot_done) {
+      count_bytes(2.0 * 4.0 * ndof);
       launch(kPdlFine, dot_kernel<float>, dim3(nb), dim3(256), 0, ndof, (const float*)K.r, (const float*)z, partials,
              (const int*)done, (const int*)nullptr, state, (int)kFinRZMixed, fin_count);
     }
+    count_bytes(3.0 * 4.0 * ndof);
     launch(kPdlFine, cg_p_kernel<float>, dim3(nb), dim3(256), 0, ndof, (const float*)z, K.p, (const PcgState*)state, 0);
     TP3D_CHECK_LAUNCH();
     return rc;
@@ -1988,6 +2106,21 @@ extern "C" int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, do
   return s->leave();
 }
 
+extern "C" int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int launches, double* ms_per_launch,
+                                      double* bytes_per_launch) {
+  if (!s || !ms_per_launch || !bytes_per_launch || launches < 1 || !s->have_density || level < 0 ||
+      level >= s->nlev - (s->nlev > 1 ? 1 : 0))
+    return TP3D_ERR_ARG;
+  if (fp32 && !s->mixed) return TP3D_ERR_ARG;
+  if (int rc = s->enter()) return rc;
+  if (!fp32 && s->mixed)
+    if (int rc = s->ensure_fp64_buffers()) return rc;
+  const int rc = fp32 ? s->time_level_cold<float>(level, launches, ms_per_launch, bytes_per_launch)
+                      : s->time_level_cold<double>(level, launches, ms_per_launch, bytes_per_launch);
+  if (rc) return rc;
+  return s->leave();
+}
+
 extern "C" int tp3d_warm_start(double* U, double* U_prev, long long n, int have_prev, void* stream) {
   if (!U || !U_prev || n < 0) return TP3D_ERR_ARG;
   if (n == 0) return TP3D_OK;
@@ -2020,7 +2153,9 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)s->cyc_L0, (s->mixed ? s->K32.loop : s->K64.loop) ? 1.0 : 0.0,
                            s->pdl ? (double)s->o.pdl : 0.0,
                            (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; }),
-                           (double)gj_status, (double)s->deep_L};
+                           (double)gj_status, (double)s->deep_L,
+                           s->mixed ? s->K32.graph_bytes : s->K64.graph_bytes,
+                           (double)(s->mixed ? s->K32.graph_kernels : s->K64.graph_kernels)};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -141,8 +141,17 @@ class HexSolver:
         keys = ["levels", "iterations", "reliable_updates", "relres", "restarts", "coarsest_dofs",
                 "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor",
                 "fp64_fallback", "fine_form_fp64", "fine_form_fp32", "fused_cycle_level", "device_loop",
-                "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level"]
+                "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level", "bytes_per_cg_iteration",
+                "kernels_per_cg_iteration"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
+
+    def time_level(self, level: int, fp32: bool, launches: int = 10):
+        """(ms per launch, algorithmic bytes per launch) of the level's operator
+        with cold L2 (tp3d_solver_time_level)."""
+        ms, nb = C.c_double(0), C.c_double(0)
+        _lib.check(_lib.lib().tp3d_solver_time_level(self._h, int(level), 1 if fp32 else 0, int(launches),
+                                                     C.byref(ms), C.byref(nb)), "time_level")
+        return ms.value, nb.value
 
 
 def get_solver(use_gpu: bool = True):
