@@ -322,7 +322,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-large", action="store_true", help="skip the 256x128x128 design")
-    ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply", "batch"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "step", "apply", "batch", "large"],
                     help="step: warm-up + --steps loop bodies only (for launch lists); "
                          "apply: fine-operator launches only (for kernel captures)")
     ap.add_argument("--size", type=int, default=NELX, help="nelx for --mode step/apply (nely = nelz = nelx/2)")
@@ -333,6 +333,8 @@ def main():
     args = ap.parse_args()
     if args.mode == "batch":
         return run_batch(args)
+    if args.mode == "large":
+        return run_large(args)
     if args.mode != "bench":
         return run_probe(args)
 
@@ -378,6 +380,23 @@ def main():
         results[prec]["accuracy"] = accuracy_vs_fp64(loop, prec)
         if prec != args.precision:
             loop.close()
+
+    # the autotuner: the same loop with the smoothing degrees searched on this
+    # grid at its first solve (the fine operator's shape and slab depth are
+    # searched at the first set_density either way), same warm-up and steps
+    tl = make_loop(args.precision, solver_options={"autotune": True})
+    for _ in range(W):
+        tl.step()
+    torch.cuda.synchronize()
+    tms, tcg, _, _ = time_device_steps(tl, args.steps, dist)
+    tms = max_over_ranks(tms, dist)
+    autotune = {"value": job_rate(args.steps, tms / 1e3, world), "unit": "iter/s",
+                "ms_per_step": tms / args.steps, "cg_iterations_per_step": tcg / args.steps,
+                "search": tl.solver.tuning,
+                "chosen": {k: v for k, v in tl.solver.stats().items()
+                           if k in ("degree_fine", "degree_level1", "degree_level2", "fine_slab_depth",
+                                    "fine_threads", "tile_y", "tile_x")}}
+    tl.close()
 
     main_r = results[args.precision]
     loop = main_r["loop"]
@@ -507,6 +526,7 @@ def main():
                           "kernels_per_cg_iteration": main_r["stats"].get("kernels_per_cg_iteration"),
                           "achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak},
         "large_design": large,
+        "autotune": autotune,
         "cpu_baseline": cpu,
         "gpu_launches": main_r["launches"],
         "clocks": clocks,
@@ -531,20 +551,101 @@ def run_batch(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     specs = batched_cantilevers(64, seed=0)
-    br = BatchRunner(specs, precision=args.precision, workers=8)
-    br.run(max(1, args.warmup))
-    conc = br.run(args.steps)
+    tuned = {}
+    for crit in ("bytes", "time"):
+        t0 = time.perf_counter()
+        br = BatchRunner(specs, precision=args.precision, workers=8, tune=crit)
+        setup_s = time.perf_counter() - t0
+        br.run(max(1, args.warmup))
+        r = br.run(args.steps)
+        r["autotune_setup_s"] = setup_s
+        r["degrees"] = [(t["degree_fine"], t["degree_level1"], t["degree_deep"]) for t in br.tuning]
+        tuned[crit] = r
+        br.close()
+    # the same position on each design's trajectory as the tuned runs (three
+    # loop bodies of tuning plus the warm-up)
+    br = BatchRunner(specs, precision=args.precision, workers=8, tune=None)
+    br.run(3 + max(1, args.warmup))
+    conc_default = br.run(args.steps)
     br.close()
-    seq = BatchRunner(specs, precision=args.precision, workers=1)
-    seq.run(max(1, args.warmup))
+    seq = BatchRunner(specs, precision=args.precision, workers=1, tune=None)
+    seq.run(3 + max(1, args.warmup))
     one = seq.run(args.steps)
     seq.close()
     nele = [s.nelx * s.nely * s.nelz for s in specs]
     print(json.dumps({"mode": "batch", "designs": len(specs), "precision": args.precision, "steps": args.steps,
                       "elements_total": int(sum(nele)), "elements_min": int(min(nele)),
-                      "elements_max": int(max(nele)), "concurrent_8_threads": conc,
-                      "one_after_another": one,
-                      "speedup": conc["simp_iterations_per_s"] / one["simp_iterations_per_s"]}))
+                      "elements_max": int(max(nele)),
+                      "concurrent_8_threads_autotuned_bytes": tuned["bytes"],
+                      "concurrent_8_threads_autotuned_time": tuned["time"],
+                      "concurrent_8_threads_default_degrees": conc_default,
+                      "one_after_another_default_degrees": one,
+                      "speedup_concurrent": conc_default["simp_iterations_per_s"] / one["simp_iterations_per_s"],
+                      "speedup_autotune_bytes": tuned["bytes"]["simp_iterations_per_s"]
+                      / conc_default["simp_iterations_per_s"],
+                      "speedup_autotune_time": tuned["time"]["simp_iterations_per_s"]
+                      / conc_default["simp_iterations_per_s"]}))
+    return 0
+
+
+def run_large(args):
+    """The large single design in full: 256x128x128 (4.19 M elements, 12.8 M
+    DOFs), volfrac 0.2, rmin 4.5, penal 3, beta 1, 2, 4, 8 with --steps loop
+    bodies per stage (default schedule: 100), mixed precision.  Each stage is
+    timed on the device with CUDA events; the compliance of the final design is
+    checked against an FP64 solve.  Prints one JSON line (not the headline bench
+    line)."""
+    import torch
+
+    from pytopo3d_b200.solver import HexSolver
+    from pytopo3d_b200.stiffness import lk_H8
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = (256, 128, 128)
+    ndof = 3 * 257 * 129 * 129
+    per_stage = args.steps
+    loop = make_loop("mixed", dims=dims, volfrac=0.2, rmin=4.5)
+    stages = []
+    total_ms, total_cg = 0.0, 0
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        with clk.timed():
+            for beta in (1.0, 2.0, 4.0, 8.0):
+                loop.set_beta(beta)
+                torch.cuda.synchronize()
+                ms, cg, launches, c = time_device_steps(loop, per_stage, None)
+                total_ms += ms
+                total_cg += cg
+                stages.append({"beta": beta, "iterations": per_stage, "ms": ms, "simp_iterations_per_s":
+                               per_stage / (ms / 1e3), "cg_iterations_per_step": cg / per_stage, "compliance": c,
+                               "kernel_launches": launches})
+    # the final design: one mixed solve against an FP64 solve to 1e-12
+    S = loop.S
+    fixed = workload(*dims)[4]
+    ref = HexSolver(*dims, lk_H8(elem_size=1.0), fixed, precision="fp64", rtol=1e-12, max_iterations=20000)
+    ref.set_density(S.rho_p, PENAL)
+    Ur = ref.solve(S.F[0], S.U[0].clone(), raise_on_fail=False)
+    loop.solver.set_density(S.rho_p, PENAL)
+    Um = loop.solver.solve(S.F[0], S.U[0].clone())
+    c_r, c_m = float(Ur @ ref.apply(Ur)), float(Um @ ref.apply(Um))
+    apply_ms = ctypes_time_apply(loop.solver, fp32=True)
+    peak, peak_kind = peaks()
+    fbytes = 8 * ndof + 4 * dims[0] * dims[1] * dims[2]
+    n_it = 4 * per_stage
+    print(json.dumps({
+        "mode": "large", "workload": "cantilever 256x128x128, void cylinder r24 (axis y), solid slab x<8, volfrac "
+                                     "0.2, rmin 4.5, beta 1/2/4/8, mixed", "iterations_per_stage": per_stage,
+        "simp_iterations_per_s": n_it / (total_ms / 1e3), "dof_cg_iters_per_s": ndof * total_cg / (total_ms / 1e3),
+        "cg_iterations_per_step": total_cg / n_it, "stages": stages,
+        "final_compliance_rel_err_vs_fp64": abs(c_m - c_r) / abs(c_r),
+        "final_displacement_rel_err_vs_fp64": float((Um - Ur).norm() / Ur.norm()),
+        "fp64_reference": {"relres": ref.last_relres, "iterations": ref.last_iterations},
+        "fine_operator": {"launch_ms": apply_ms, "bytes_per_launch": fbytes,
+                          "achieved_gbs": fbytes / (apply_ms * 1e-3) / 1e9,
+                          "frac": fbytes / (apply_ms * 1e-3) / 1e9 / peak, "peak": peak, "peak_source": peak_kind},
+        "solver": loop.solver.stats(), "clocks": clk.summary(),
+        "device_memory_in_use_gb": (lambda fm: (fm[1] - fm[0]) / 1e9)(torch.cuda.mem_get_info())}))
+    ref.close()
+    loop.close()
     return 0
 
 

@@ -294,6 +294,24 @@ int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
  * counterpart. */
 int tp3d_solver_time_apply(tp3d_solver* s, int fp32, int launches, double* ms_per_launch);
 
+/* Autotuner of the smoothing degrees: a coordinate search from the current setting over the
+ * deeper levels' Chebyshev degree (2, 4, 6), then level 1's (1, 2, 3), then the fine level's
+ * (1, 2).  A candidate's cost is its solve of K U = F from the initial guess U0 (device, not
+ * modified): criterion 0 (latency: one design alone on the GPU) the faster of two solves timed
+ * on the host clock after a first one that captures the iteration graph; criterion 1
+ * (throughput: designs sharing the GPU) the solve's algorithmic bytes, CG iterations times the
+ * bytes of one iteration.  The cheapest candidate that converged (without the mixed form's FP64
+ * fallback) becomes the solver's setting.  Call it on a representative design and warm start
+ * (the SIMP loop does so at an iteration of the caller's choice).  The choice is cached per
+ * process for the grid, precision and criterion: a later call applies it without solving.  (The
+ * fine operator's launch shape and slab depth are chosen by timing at the first set_density and
+ * cached the same way.)  report (host, up to 10 doubles): fine, level-1 and deeper degrees
+ * chosen, best and starting-setting cost (ms for criterion 0, GB for criterion 1), candidates
+ * tried, 1 when taken from the cache, the criterion, the CG iterations and bytes per iteration of
+ * the last candidate solved.  No reference counterpart. */
+int tp3d_solver_autotune(tp3d_solver* s, const double* F, const double* U0, int criterion, double* report,
+                         int nreport);
+
 /* Average device time (ms) of one Apply-mode launch of the level-`level` operator (0: the fine
  * operator; >= 1: the coarse packed-stencil kernel of the V-cycle; the coarsest dense level is
  * excluded), each launch timed alone with its own CUDA events after a 256 MiB write that evicts
@@ -315,7 +333,10 @@ int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int launches, do
  * with the coarsest solve (0 none), the algorithmic bytes of one CG iteration (every array each
  * kernel of the iteration must read or write once, summed over the iteration's kernels; the
  * reliable-update branch excluded; 0 before the first solve), the kernels launched per CG
- * iteration.  Returns the count written. */
+ * iteration, the autotuner state (0 not tuned, 1 searched, 2 from the cache), the smoothing degrees
+ * of the fine level, level 1 and level 2, the fine operator's slab depth (node planes per block; 0
+ * for the dense form) and threads per block of the Walsh-Hadamard form in use.  Returns the count
+ * written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* Initial guess for the next solve of a load case from its last two solutions:

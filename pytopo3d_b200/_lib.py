@@ -93,6 +93,7 @@ SIGNATURES = {
     "tp3d_solver_apply_f64": (i32, [vp, vp, vp]),
     "tp3d_solver_apply_f32": (i32, [vp, vp, vp]),
     "tp3d_solver_time_apply": (i32, [vp, i32, i32, C.POINTER(f64)]),
+    "tp3d_solver_autotune": (i32, [vp, vp, vp, i32, C.POINTER(f64), i32]),
     "tp3d_solver_time_level": (i32, [vp, i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),
     "tp3d_solver_stats": (i32, [vp, C.POINTER(f64), i32]),
     "tp3d_warm_start": (i32, [vp, vp, i64, i32, vp]),

@@ -101,10 +101,15 @@ def design_problem(spec: DesignSpec):
 class BatchRunner:
     """One ``SimpLoop`` per design on its own stream; ``run(iterations)``
     advances every design by that many loop bodies with ``workers`` host
-    threads (design i is always driven by thread i % workers)."""
+    threads (design i is always driven by thread i % workers).  With ``tune``
+    ("bytes", the default, or "time"; None: off) every design first runs three
+    loop bodies alone, the third of which autotunes its smoothing degrees on its
+    own grid (``HexSolver.autotune``).  The designs then share the GPU, where
+    throughput counts, so the default criterion is the solve's traffic."""
 
     def __init__(self, specs: List[DesignSpec], precision: str = "mixed", beta: float = 1.0, eta: float = 0.5,
-                 move: float = 0.2, workers: int = 8, solver_options: Optional[dict] = None):
+                 move: float = 0.2, workers: int = 8, solver_options: Optional[dict] = None,
+                 tune: Optional[str] = "bytes"):
         self.specs = list(specs)
         self.workers = max(1, min(int(workers), len(self.specs)))
         # the designs already run side by side: each solver's set-up keeps its
@@ -127,6 +132,20 @@ class BatchRunner:
 
         self._each(build)
         torch.cuda.synchronize()
+        if tune:
+            # smoothing degrees per design, searched at each design's third loop
+            # body, one design at a time so that no other design's work disturbs
+            # the timings (cached per grid)
+            self.tuning = []
+            for i, loop in enumerate(self.loops):
+                loop.solver.autotune_at = 3
+                loop.solver.autotune_pending = True
+                loop.solver.autotune_criterion = tune
+                with torch.cuda.stream(self.streams[i]):
+                    for _ in range(3):
+                        loop.step()
+                torch.cuda.synchronize()
+                self.tuning.append(loop.solver.tuning)
         self.cg_iterations = [0] * len(self.specs)
         self.compliance = [float("nan")] * len(self.specs)
 

@@ -19,8 +19,12 @@
 // the coarsest level is a dense inverse.  One CG iteration is captured once
 // into a CUDA graph and replayed; the host polls the stop flag between replays.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "tp3d_fine.cuh"
@@ -64,6 +68,44 @@ double op_bytes(long long n, long long nn, double src) {
 constexpr int kMaxPartials = 1 << 16;
 constexpr int kSpectraPartials = 4096;  // per level at set-up: two reductions of at most 2048 blocks
 constexpr int kPdlCoarse = 1, kPdlFine = 2;  // tp3d_solver_opts::pdl bits
+
+// Process-wide caches of tuning choices (fine operator form and tile; the
+// smoothing degrees of the autotuner), keyed by the grid and precision.
+struct FineChoiceKey {
+  int nx, ny, nz, tsize, bf16, form_opt;
+  bool operator<(const FineChoiceKey& o) const {
+    return std::tie(nx, ny, nz, tsize, bf16, form_opt) < std::tie(o.nx, o.ny, o.nz, o.tsize, o.bf16, o.form_opt);
+  }
+};
+struct FineChoice {
+  bool use;
+  WhtTile tile;
+};
+inline std::mutex& fine_choice_mu() {
+  static std::mutex m;
+  return m;
+}
+inline std::map<FineChoiceKey, FineChoice>& fine_choice_cache() {
+  static std::map<FineChoiceKey, FineChoice> c;
+  return c;
+}
+struct DegreeKey {
+  int nx, ny, nz, mixed;
+  bool operator<(const DegreeKey& o) const {
+    return std::tie(nx, ny, nz, mixed) < std::tie(o.nx, o.ny, o.nz, o.mixed);
+  }
+};
+struct Degrees {
+  int fine, coarse, deep;
+};
+inline std::mutex& degree_mu() {
+  static std::mutex m;
+  return m;
+}
+inline std::map<DegreeKey, Degrees>& degree_cache() {
+  static std::map<DegreeKey, Degrees> c;
+  return c;
+}
 
 template <typename T>
 struct LevelVec {
@@ -544,48 +586,87 @@ struct tp3d_solver {
   }
 
   // Fine operator form for precision T: the dense-KE kernel or one of the
-  // Walsh-Hadamard variants, whichever runs the Apply mode fastest on this
-  // grid with cold inputs (time_fine_cold, 12 launches each);
-  // fine_operator = 1 / 2 restricts the choice to one form.
+  // Walsh-Hadamard launch shapes, whichever runs the Apply mode fastest on this
+  // grid with cold inputs (time_fine_cold, 8 launches each).  For each shape
+  // (threads per block, hence the node patch and elements per block) the slab
+  // depth (node planes per block along z) is searched too: the tile model's
+  // choice, half of it and twice it.  fine_operator = 1 / 2 restricts the
+  // choice to one form, 3..5 to one shape.  The choice is cached per process
+  // for the grid, precision and modulus source, so later solvers of the same
+  // grid skip the timing.
+  template <typename T>
+  WhtTile wht_tile_for(int v) const {
+    if constexpr (sizeof(T) == 8) return wht_choose_tile<double, EFromF64>(g, nsm, v);
+    else if (rho16) return wht_choose_tile<float, EFromBF16>(g, nsm, v);
+    else return wht_choose_tile<float, EFromF32>(g, nsm, v);
+  }
   template <typename T>
   int choose_fine_form() {
     bool& use = sizeof(T) == 8 ? use_wht64 : use_wht32;
     WhtTile& wt = sizeof(T) == 8 ? wt64 : wt32;
     use = false;
     if (!wht_ok) return TP3D_OK;
-    auto time_one = [&](double* ms) -> int { return time_fine_cold<T>(12, ms); };
+    const FineChoiceKey key{g.nx, g.ny, g.nz, (int)sizeof(T), rho16 ? 1 : 0, o.fine_operator};
+    {
+      std::lock_guard<std::mutex> lk(fine_choice_mu());
+      auto it = fine_choice_cache().find(key);
+      if (it != fine_choice_cache().end()) {
+        use = it->second.use;
+        wt = it->second.tile;
+        return TP3D_OK;
+      }
+    }
+    auto time_one = [&](double* ms) -> int { return time_fine_cold<T>(8, ms); };
     double best = 1e300;
-    int best_v = -1;
+    WhtTile best_t;
+    bool best_wht = false;
     int rc = TP3D_OK;
     if (o.fine_operator == 0) rc = time_one(&best);  // dense form
+    const int NZ = g.nz + 1;
     for (int v = 0; v < kWhtVariants && rc == TP3D_OK; ++v) {
       if (o.fine_operator > 2 && v != o.fine_operator - 3) continue;
-      WhtTile w;
-      if constexpr (sizeof(T) == 8) w = wht_choose_tile<double, EFromF64>(g, nsm, v);
-      else if (rho16) w = wht_choose_tile<float, EFromBF16>(g, nsm, v);
-      else w = wht_choose_tile<float, EFromF32>(g, nsm, v);
-      if ((long long)w.tiles_y * w.tiles_x * w.zchunks > kMaxPartials) continue;
-      wt = w;
-      use = true;
-      double ms = 0.0;
-      rc = time_one(&ms);
-      use = false;
-      if (rc == TP3D_OK && ms < best) {
-        best = ms;
-        best_v = v;
+      const WhtTile base = wht_tile_for<T>(v);
+      int zcs[3] = {base.ZC, std::max(1, base.ZC / 2), std::min(NZ, 2 * base.ZC)};
+      for (int k = 0; k < 3 && rc == TP3D_OK; ++k) {
+        if (k > 0 && (zcs[k] == base.ZC || (k == 2 && zcs[2] == zcs[1]))) continue;
+        WhtTile w = base;
+        w.ZC = zcs[k];
+        w.zchunks = (NZ + w.ZC - 1) / w.ZC;
+        if ((long long)w.tiles_y * w.tiles_x * w.zchunks > kMaxPartials) continue;
+        wt = w;
+        use = true;
+        double ms = 0.0;
+        rc = time_one(&ms);
+        use = false;
+        if (rc == TP3D_OK && ms < best) {
+          best = ms;
+          best_t = w;
+          best_wht = true;
+        }
       }
     }
     if (rc) return rc;
-    if (best_v >= 0) {
-      if constexpr (sizeof(T) == 8) wt = wht_choose_tile<double, EFromF64>(g, nsm, best_v);
-      else if (rho16) wt = wht_choose_tile<float, EFromBF16>(g, nsm, best_v);
-      else wt = wht_choose_tile<float, EFromF32>(g, nsm, best_v);
+    if (best_wht) {
+      wt = best_t;
       use = true;
     }
+    std::lock_guard<std::mutex> lk(fine_choice_mu());
+    fine_choice_cache()[key] = FineChoice{use, wt};
     return TP3D_OK;
   }
 
-
+  // ---------------- autotuning of the smoothing degrees ----------------
+  // Drop the CG iteration graphs: the next solve captures them again with the
+  // current options (the smoothing degrees are read at capture).
+  void drop_graphs() {
+    for (auto* K : {&K64.graph, &K32.graph})
+      if (*K) {
+        cudaGraphExecDestroy(*K);
+        *K = nullptr;
+      }
+    K64.loop = K32.loop = false;
+  }
+  int tuned = 0;  // 0 not tuned, 1 searched here, 2 taken from the cache
 
   template <typename T, int MODE>
   int apply_level(int L, const OpIO<T>& io) {
@@ -2121,6 +2202,137 @@ extern "C" int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int l
   return s->leave();
 }
 
+// Smoothing degrees by measurement, a coordinate search from the current
+// setting: the deeper levels' degree (2, 4, 6), then level 1's (1, 2, 3) with
+// the best of those, then the fine level's (1, 2).  The cost of a candidate is
+// its solve of K U = F from U0:
+//   criterion 0 (latency, one design on the GPU): the faster of two timed
+//     solves (after a first one that captures the iteration graph), on the host
+//     clock around the whole solve, its host wait included;
+//   criterion 1 (throughput, designs sharing the GPU): the solve's algorithmic
+//     bytes, CG iterations times the bytes of one iteration (one solve).
+// The cheapest candidate that converged without the mixed form's FP64
+// fallback is kept.  The choice is cached per process for the grid, precision
+// and criterion; a later call applies it without solving.
+extern "C" int tp3d_solver_autotune(tp3d_solver* s, const double* F, const double* U0, int criterion,
+                                    double* report, int nreport) {
+  if (!s || !F || !U0 || (nreport > 0 && !report)) return TP3D_ERR_ARG;
+  if (!s->have_density) {
+    tp3d_set_last_error("tp3d_solver_set_density must be called before autotune");
+    return TP3D_ERR_ARG;
+  }
+  if (s->o.smoother == 1) {
+    tp3d_set_last_error("autotune searches Chebyshev degrees; the damped-Jacobi smoother has none");
+    return TP3D_ERR_ARG;
+  }
+  if (criterion != 0 && criterion != 1) {
+    tp3d_set_last_error("autotune criterion must be 0 (solve time) or 1 (solve bytes)");
+    return TP3D_ERR_ARG;
+  }
+  const DegreeKey key{s->g.nx, s->g.ny, s->g.nz, (s->mixed ? 1 : 0) + 2 * criterion};
+  auto apply = [&](const Degrees& d) {
+    s->o.pre_sweeps = s->o.post_sweeps = d.fine;
+    s->o.coarse_sweeps = d.coarse;
+    s->o.deep_sweeps = d.deep;
+    s->o.block_sweeps = 0;
+    s->drop_graphs();
+  };
+  std::vector<double> rep(10, 0.0);
+  {
+    std::lock_guard<std::mutex> lk(degree_mu());
+    auto it = degree_cache().find(key);
+    if (it != degree_cache().end()) {
+      apply(it->second);
+      s->tuned = 2;
+      rep = {(double)it->second.fine, (double)it->second.coarse, (double)it->second.deep, 0, 0, 0, 1,
+             (double)criterion, 0, 0};
+      for (int i = 0; i < std::min<int>(nreport, (int)rep.size()); ++i) report[i] = rep[i];
+      return TP3D_OK;
+    }
+  }
+  const long long ndof = 3 * s->g.nnode();
+  double* U = nullptr;
+  if (cudaMalloc(&U, ndof * sizeof(double)) != cudaSuccess) {
+    tp3d_set_last_error("autotune: allocation failed");
+    return TP3D_ERR_CUDA;
+  }
+  struct Free {
+    double* p;
+    ~Free() { cudaFree(p); }
+  } guard{U};
+  const Degrees start{s->o.pre_sweeps, s->pre_sweeps(1), s->pre_sweeps(2)};
+  // U0 and F may still be in flight on the caller's stream: the copies below
+  // run on the solver's stream, so order it after the caller's work first
+  if (int e = s->enter()) return e;
+  auto run = [&](double* sec) -> int {
+    TP3D_CHECK(cudaMemcpyAsync(U, U0, ndof * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    const auto t0 = std::chrono::steady_clock::now();
+    int it = 0;
+    double rr = 0.0;
+    const int rc = tp3d_solver_solve(s, F, U, &it, &rr);
+    *sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc == TP3D_OK && s->last_fallback) return TP3D_NOT_CONVERGED;
+    return rc;
+  };
+  std::map<std::tuple<int, int, int>, double> seen;
+  int tried = 0;
+  int last_cost_iters = 0;
+  double last_cost_bytes = 0.0;
+  // time of a candidate (infinite if it did not converge); <0 on a CUDA error
+  auto measure = [&](const Degrees& d, double* t) -> int {
+    auto k = std::make_tuple(d.fine, d.coarse, d.deep);
+    auto it = seen.find(k);
+    if (it != seen.end()) {
+      *t = it->second;
+      return TP3D_OK;
+    }
+    apply(d);
+    double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    int rc = run(&t1);
+    if (criterion == 0) {
+      if (rc == TP3D_OK) rc = run(&t2);
+      if (rc == TP3D_OK) rc = run(&t3);
+    }
+    ++tried;
+    if (rc < 0 && rc != TP3D_ERR_NONFINITE) return rc;
+    const double bytes = (double)s->last_iters * (s->mixed ? s->K32.graph_bytes : s->K64.graph_bytes);
+    *t = rc != TP3D_OK ? INFINITY : criterion == 0 ? std::min(t2, t3) * 1e3 : bytes * 1e-9;
+    last_cost_iters = s->last_iters;
+    last_cost_bytes = s->mixed ? s->K32.graph_bytes : s->K64.graph_bytes;
+    seen[k] = *t;
+    return TP3D_OK;
+  };
+  Degrees best_d = start;
+  double best = INFINITY, t_start = INFINITY;
+  if (int rc = measure(start, &t_start)) return rc;
+  best = t_start;
+  for (int pass = 0; pass < 3; ++pass) {
+    const std::vector<int> values = pass == 0 ? std::vector<int>{2, 4, 6}
+                                    : pass == 1 ? std::vector<int>{1, 2, 3} : std::vector<int>{1, 2};
+    const Degrees base = best_d;
+    for (int v : values) {
+      Degrees d = base;
+      (pass == 0 ? d.deep : pass == 1 ? d.coarse : d.fine) = v;
+      double t = 0.0;
+      if (int rc = measure(d, &t)) return rc;
+      if (t < best) {
+        best = t;
+        best_d = d;
+      }
+    }
+  }
+  apply(best_d);
+  s->tuned = 1;
+  {
+    std::lock_guard<std::mutex> lk(degree_mu());
+    degree_cache()[key] = best_d;
+  }
+  rep = {(double)best_d.fine, (double)best_d.coarse, (double)best_d.deep, best, t_start, (double)tried,
+         0, (double)criterion, (double)last_cost_iters, last_cost_bytes};
+  for (int i = 0; i < std::min<int>(nreport, (int)rep.size()); ++i) report[i] = rep[i];
+  return TP3D_OK;
+}
+
 extern "C" int tp3d_warm_start(double* U, double* U_prev, long long n, int have_prev, void* stream) {
   if (!U || !U_prev || n < 0) return TP3D_ERR_ARG;
   if (n == 0) return TP3D_OK;
@@ -2155,7 +2367,11 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)std::count_if(s->S16.begin(), s->S16.end(), [](const void* p) { return p; }),
                            (double)gj_status, (double)s->deep_L,
                            s->mixed ? s->K32.graph_bytes : s->K64.graph_bytes,
-                           (double)(s->mixed ? s->K32.graph_kernels : s->K64.graph_kernels)};
+                           (double)(s->mixed ? s->K32.graph_kernels : s->K64.graph_kernels),
+                           (double)s->tuned, (double)s->o.pre_sweeps, (double)s->pre_sweeps(1),
+                           (double)s->pre_sweeps(2),
+                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.ZC : 0) : (s->use_wht64 ? s->wt64.ZC : 0)),
+                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.nthr : 0) : (s->use_wht64 ? s->wt64.nthr : 0))};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -136,6 +136,7 @@ class SimpState:
         self.U = torch.zeros_like(F)
         self.U_prev = torch.zeros_like(F)  # last solutions, for the extrapolated initial guess
         self.n_solved = 0
+        self.n_iter = 0  # loop bodies run (not reset between stages)
         self.sens_scratch = torch.empty(
             _lib.lib().tp3d_sensitivity_scratch_bytes(H.nelx, H.nely, H.nelz), dtype=torch.uint8,
             device=device())
@@ -162,6 +163,8 @@ class SimpState:
             _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
                                          1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
             dst_dc = self.dc_dx if k == 0 else self.dc_acc
+            if k == 0 and self.solver.autotune_pending and self.n_iter + 1 >= self.solver.autotune_at:
+                self.solver.autotune(self.F[k], self.U[k])
 
             def sens():
                 _lib.check(L.tp3d_sensitivity(
@@ -182,6 +185,7 @@ class SimpState:
                 self.dc_dx += self.dc_acc
                 self.c_dev[0] += self.c_dev[1]
         self.n_solved += 1
+        self.n_iter += 1
         return iters
 
 

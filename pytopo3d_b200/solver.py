@@ -47,6 +47,16 @@ class HexSolver:
         self.ndof = 3 * (nelx + 1) * (nely + 1) * (nelz + 1)
         self.nele = nelx * nely * nelz
         self.precision = precision
+        # autotune=k: a SIMP loop searches the smoothing degrees at its k-th
+        # iteration (True: the third), on that iteration's design and warm start
+        # (tp3d_solver_autotune); the choice is cached per grid and precision
+        at = opts.pop("autotune", 0)
+        self.autotune_at = 3 if at is True else int(at or 0)
+        self.autotune_pending = self.autotune_at > 0
+        # "time": fastest solve alone on the GPU; "bytes": least solve traffic
+        # (designs that share the GPU, where throughput rather than latency counts)
+        self.autotune_criterion = opts.pop("autotune_criterion", "time")
+        self.tuning = None
         L = _lib.lib()
         o = _lib.SolverOpts()
         L.tp3d_solver_default_opts(C.byref(o))
@@ -142,8 +152,26 @@ class HexSolver:
                 "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor",
                 "fp64_fallback", "fine_form_fp64", "fine_form_fp32", "fused_cycle_level", "device_loop",
                 "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level", "bytes_per_cg_iteration",
-                "kernels_per_cg_iteration"]
+                "kernels_per_cg_iteration", "autotuned", "degree_fine", "degree_level1", "degree_level2",
+                "fine_slab_depth", "fine_threads"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
+
+    def autotune(self, F: torch.Tensor, U0: Optional[torch.Tensor] = None, criterion: Optional[str] = None) -> dict:
+        """Search the smoothing degrees on this grid (tp3d_solver_autotune) with
+        K U = F from U0; criterion "time" (default) or "bytes"; returns the choice
+        and the costs (ms for "time", GB for "bytes")."""
+        F = vec(F)
+        U0 = torch.zeros_like(F) if U0 is None else U0
+        crit = {"time": 0, "bytes": 1}[criterion or self.autotune_criterion]
+        rep = (C.c_double * 10)()
+        _lib.check(_lib.lib().tp3d_solver_autotune(self._h, F.data_ptr(), U0.data_ptr(), crit, rep, 10),
+                   "autotune")
+        self.autotune_pending = False
+        self.tuning = {"degree_fine": int(rep[0]), "degree_level1": int(rep[1]), "degree_deep": int(rep[2]),
+                       "best": rep[3], "start": rep[4], "tried": int(rep[5]), "from_cache": bool(rep[6]),
+                       "criterion": ("time", "bytes")[crit], "last_iterations": int(rep[8]),
+                       "last_bytes_per_iteration": rep[9]}
+        return self.tuning
 
     def time_level(self, level: int, fp32: bool, launches: int = 10):
         """(ms per launch, algorithmic bytes per launch) of the level's operator

@@ -31,7 +31,7 @@ def test_concurrent_designs_match_sequential_runs():
 
     specs = batched_cantilevers(6, seed=1)
     opts = {"fine_operator": 3}
-    br = BatchRunner(specs, precision="fp64", workers=3, solver_options=opts)
+    br = BatchRunner(specs, precision="fp64", workers=3, solver_options=opts, tune=None)
     stats = br.run(2)
     assert stats["designs"] == 6 and stats["simp_iterations_per_s"] > 0
     KE = lk_H8(elem_size=1.0)
@@ -46,4 +46,20 @@ def test_concurrent_designs_match_sequential_runs():
         assert c == pytest.approx(br.compliance[i], rel=1e-10), i
         np.testing.assert_allclose(loop.design().cpu().numpy(), br.design(i).cpu().numpy(), rtol=0, atol=1e-10)
         loop.close()
+    br.close()
+
+
+def test_batch_designs_are_autotuned_one_by_one():
+    """With tuning on (the default), every design gets smoothing degrees searched
+    on its own grid, and the batch still runs."""
+    from pytopo3d_b200.batch import BatchRunner, batched_cantilevers
+
+    specs = batched_cantilevers(3, seed=7)
+    br = BatchRunner(specs, precision="mixed", workers=3)
+    assert len(br.tuning) == 3
+    for t, loop in zip(br.tuning, br.loops):
+        assert t["degree_fine"] in (1, 2) and t["degree_deep"] in (2, 4, 6)
+        assert loop.solver.stats()["autotuned"] in (1, 2)
+    stats = br.run(2)
+    assert np.isfinite(br.compliance).all() and stats["dof_cg_iterations_per_s"] > 0
     br.close()

@@ -456,3 +456,43 @@ def test_nonfinite_density_reports_an_error_not_a_hang(P):
     with pytest.raises(RuntimeError):
         s.solve(F)
     s.close()
+
+
+@pytest.mark.parametrize("precision,criterion", [("fp64", "time"), ("mixed", "time"), ("mixed", "bytes")])
+def test_autotune_picks_measured_degrees_and_caches_them(P, precision, criterion):
+    """tp3d_solver_autotune searches the smoothing degrees by timing solves on
+    the grid at hand (a coordinate search of at most 7 candidates), keeps the
+    fastest, records it in stats(), caches it per (grid, precision), and
+    leaves the solution unchanged within the solver's tolerance."""
+    from pytopo3d_b200.solver import HexSolver
+    from pytopo3d_b200._tensors import to_flat
+
+    nx, ny, nz = 26, 13, 11  # a grid no other test tunes (the cache is per grid, precision, criterion)
+    rho, free, fmask = _problem(nx, ny, nz, seed=4, lo=0.05)
+    KE = P.lk_H8(elem_size=1.0)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, ndof)).cuda()
+    rd = to_flat(rho)
+    ref = HexSolver(nx, ny, nz, KE, fmask, precision=precision)
+    ref.set_density(rd, 3.0)
+    U_ref = ref.solve(F)
+    s = HexSolver(nx, ny, nz, KE, fmask, precision=precision)
+    s.set_density(rd, 3.0)
+    t = s.autotune(F, criterion=criterion)
+    assert not t["from_cache"] and 1 <= t["tried"] <= 7
+    assert t["degree_fine"] in (1, 2) and t["degree_level1"] in (1, 2, 3) and t["degree_deep"] in (2, 4, 6)
+    assert 0 < t["best"] <= t["start"], t
+    st = s.stats()
+    assert st["autotuned"] == 1 and st["degree_fine"] == t["degree_fine"]
+    assert st["degree_level1"] == t["degree_level1"] and st["degree_level2"] == t["degree_deep"]
+    U = s.solve(F)
+    tol = 1e-8 if precision == "fp64" else 1e-5
+    assert float((U - U_ref).norm() / U_ref.norm()) <= tol
+    s2 = HexSolver(nx, ny, nz, KE, fmask, precision=precision)
+    s2.set_density(rd, 3.0)
+    t2 = s2.autotune(F, criterion=criterion)
+    assert t2["from_cache"] and (t2["degree_fine"], t2["degree_level1"], t2["degree_deep"]) == (
+        t["degree_fine"], t["degree_level1"], t["degree_deep"])
+    assert s2.stats()["autotuned"] == 2
+    for h in (ref, s, s2):
+        h.close()
