@@ -199,10 +199,13 @@ typedef struct tp3d_solver_opts {
   double reliable_delta;/* mixed: replace the FP32 residual by the FP64 one when it fell by this factor */
   int max_restarts;     /* FP64: restarts from the true residual when the recursive one drifted */
   int fine_operator;    /* fine-level K u: 0 the fastest of the dense-KE form and the Walsh-Hadamard
-                           block form's launch shapes, timed on the grid at the first set_density;
-                           1 dense KE; 2 Walsh-Hadamard (fastest shape); 3, 4, 5 Walsh-Hadamard with
-                           shape 0, 1, 2.  The block form needs an axis-aligned orthotropic KE and
-                           falls back to the dense form otherwise. */
+                           block form's launch shapes and slab depths, timed on the grid at the first
+                           set_density; 1 dense KE; 2 Walsh-Hadamard (fastest shape); 3 + v the
+                           Walsh-Hadamard form with shape v only (FP64: v = 0..2; FP32: v = 0..2 the
+                           packed two-plane kernel with paired FP32 instructions, 3..5 the scalar
+                           kernel; the timed choices 0 and 2 consider only the scalar FP32 shapes,
+                           which measured faster).  The block form needs an axis-aligned orthotropic
+                           KE and falls back to the dense form otherwise. */
   int fused_cycle_dofs; /* the V-cycle from the first level (>= 1) with at most this many DOFs down
                            to the coarsest runs as one cooperative launch with grid barriers;
                            0 (default) keeps one launch per smoothing step and transfer, which

@@ -5,6 +5,7 @@
 #include <cmath>
 
 #include "tp3d_fine_wht.cuh"
+#include "tp3d_fine_wht2.cuh"
 
 namespace tp3d {
 
@@ -13,15 +14,28 @@ namespace {
 // (threads, min blocks per SM) of each variant, per precision
 template <typename T>
 struct WhtShapes;
+// FP32 offers the packed two-plane kernel (tp3d_fine_wht2.cuh, twice the scalar
+// kernel's per-thread state, so fewer threads per block) and the scalar one
+// variants 0-2 the packed kernel, 3-5 the scalar one (both are timed)
 template <>
 struct WhtShapes<float> {
-  static constexpr int nthr[kWhtVariants] = {512, 768, 256};
-  static constexpr int minb[kWhtVariants] = {2, 1, 4};
+  static constexpr int count = 6;
+  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 512, 768, 256};
+  static constexpr int minb[kWhtVariants] = {1, 1, 3, 2, 1, 4};
+  static constexpr bool packed[kWhtVariants] = {true, true, true, false, false, false};
 };
+
+// dynamic shared memory of a launch of variant v
+template <typename T>
+constexpr size_t wht_kernel_smem(int v) {
+  return WhtShapes<T>::packed[v] ? wht2_smem_bytes(WhtShapes<T>::nthr[v]) : wht_smem_bytes<T>(WhtShapes<T>::nthr[v]);
+}
 template <>
 struct WhtShapes<double> {
-  static constexpr int nthr[kWhtVariants] = {256, 384, 128};
-  static constexpr int minb[kWhtVariants] = {2, 1, 4};
+  static constexpr int count = 3;
+  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 256, 384, 128};
+  static constexpr int minb[kWhtVariants] = {2, 1, 4, 2, 1, 4};
+  static constexpr bool packed[kWhtVariants] = {false, false, false, false, false, false};
 };
 
 template <typename T, class ESrc, int V>
@@ -30,7 +44,8 @@ struct WhtVariant {
   static constexpr int MINB = WhtShapes<T>::minb[V];
   template <int MODE>
   static void* fn() {
-    return (void*)wht_apply_kernel<T, ESrc, MODE, NTHR, MINB>;
+    if constexpr (WhtShapes<T>::packed[V]) return (void*)wht2_apply_kernel<ESrc, MODE, NTHR, MINB>;
+    else return (void*)wht_apply_kernel<T, ESrc, MODE, NTHR, MINB>;
   }
   static void* by_mode(int mode) {
     switch (mode) {
@@ -48,6 +63,14 @@ struct WhtVariant {
 
 template <typename T, class ESrc>
 void* wht_fn(int mode, int v) {
+  if constexpr (WhtShapes<T>::count > 3) {
+    switch (v) {
+      case 3: return WhtVariant<T, ESrc, 3>::by_mode(mode);
+      case 4: return WhtVariant<T, ESrc, 4>::by_mode(mode);
+      case 5: return WhtVariant<T, ESrc, 5>::by_mode(mode);
+      default: break;
+    }
+  }
   switch (v) {
     case 0: return WhtVariant<T, ESrc, 0>::by_mode(mode);
     case 1: return WhtVariant<T, ESrc, 1>::by_mode(mode);
@@ -59,7 +82,7 @@ void* wht_fn(int mode, int v) {
 template <typename T, class ESrc>
 bool wht_prepare(int v) {
   const int nthr = WhtShapes<T>::nthr[v];
-  const int smem = (int)wht_smem_bytes<T>(nthr);
+  const int smem = (int)wht_kernel_smem<T>(v);
   for (int mode = 0; mode <= kModeChebStepDot; ++mode)
     if (ensure_dynamic_smem(wht_fn<T, ESrc>(mode, v), smem) != TP3D_OK) return false;
   return true;
@@ -73,22 +96,27 @@ int wht_variant_threads(int v) {
 }
 
 template <typename T, class ESrc>
+int wht_variant_count() {
+  return WhtShapes<T>::count;
+}
+
+template <typename T, class ESrc>
 int wht_occupancy(int v) {
   if (!wht_prepare<T, ESrc>(v)) return 1;
   int occ = 0;
   const int nthr = WhtShapes<T>::nthr[v];
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wht_fn<T, ESrc>(kModeChebStep, v), nthr,
-                                                wht_smem_bytes<T>(nthr));
+                                                wht_kernel_smem<T>(v));
   return std::max(occ, 1);
 }
 
 template <typename T, class ESrc>
 int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStream_t st, bool pdl) {
-  if (v < 0 || v >= kWhtVariants || !wht_prepare<T, ESrc>(v)) return TP3D_ERR_ARG;
+  if (v < 0 || v >= WhtShapes<T>::count || !wht_prepare<T, ESrc>(v)) return TP3D_ERR_ARG;
   const int nthr = WhtShapes<T>::nthr[v];
   void* args[] = {(void*)&p};
-  const cudaError_t e = launch_kernel_c(pdl, wht_fn<T, ESrc>(mode, v), grid, dim3(nthr), wht_smem_bytes<T>(nthr), st,
-                                        args);
+  const cudaError_t e = launch_kernel_c(pdl, wht_fn<T, ESrc>(mode, v), grid, dim3(nthr), wht_kernel_smem<T>(v),
+                                        st, args);
   return e == cudaSuccess ? TP3D_OK : TP3D_ERR_CUDA;
 }
 
@@ -176,6 +204,7 @@ WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
 
 #define TP3D_WHT_INSTANTIATE(T, ESrc)                                                     \
   template int wht_variant_threads<T, ESrc>(int);                                        \
+  template int wht_variant_count<T, ESrc>();                                             \
   template int wht_occupancy<T, ESrc>(int);                                              \
   template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t, bool); \
   template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);

@@ -247,9 +247,11 @@ __global__ void __launch_bounds__(NTHR, MINB) wht_apply_kernel(const __grid_cons
 namespace tp3d {
 
 // Block shapes offered for the Walsh-Hadamard operator (threads, minimum
-// resident blocks per SM).  Explicit instantiations live in tp3d_fine_wht.cu;
-// the solver times them on its own grid and keeps the fastest.
-constexpr int kWhtVariants = 3;
+// resident blocks per SM; for FP32 the packed two-plane kernel and the scalar
+// one).  Explicit instantiations live in tp3d_fine_wht.cu; the solver times
+// them on its own grid and keeps the fastest.  kWhtVariants is the most any
+// precision offers (wht_variant_count).
+constexpr int kWhtVariants = 6;
 
 // Host view of one launch configuration.
 struct WhtTile {
@@ -259,6 +261,8 @@ struct WhtTile {
 
 template <typename T, class ESrc>
 int wht_variant_threads(int v);
+template <typename T, class ESrc>
+int wht_variant_count();
 template <typename T, class ESrc>
 int wht_occupancy(int v);
 template <typename T, class ESrc>

@@ -623,8 +623,15 @@ struct tp3d_solver {
     int rc = TP3D_OK;
     if (o.fine_operator == 0) rc = time_one(&best);  // dense form
     const int NZ = g.nz + 1;
-    for (int v = 0; v < kWhtVariants && rc == TP3D_OK; ++v) {
+    int nvar;
+    if constexpr (sizeof(T) == 8) nvar = wht_variant_count<double, EFromF64>();
+    else nvar = wht_variant_count<float, EFromF32>();
+    for (int v = 0; v < nvar && rc == TP3D_OK; ++v) {
       if (o.fine_operator > 2 && v != o.fine_operator - 3) continue;
+      // the packed FP32 shapes (0-2) are taken only when asked for by name: on
+      // B200 they measured slower than the scalar ones (150 registers per thread,
+      // a quarter of the resident warps), so the timed choice skips them
+      if (o.fine_operator <= 2 && nvar > 3 && v < 3) continue;
       const WhtTile base = wht_tile_for<T>(v);
       int zcs[3] = {base.ZC, std::max(1, base.ZC / 2), std::min(NZ, 2 * base.ZC)};
       for (int k = 0; k < 3 && rc == TP3D_OK; ++k) {

@@ -80,6 +80,40 @@ def test_apply_matches_assembled_matrix(P, dims, form):
     s.close()
 
 
+# FP32 Walsh-Hadamard shapes: 0-2 the packed two-plane kernel (paired FP32
+# instructions), 3-5 the scalar kernel.  Odd plane counts per block and grids
+# spanning several tiles and z chunks; the apply against the assembled FP64
+# operator, and a mixed solve (every epilogue mode of the kernel) against FP64.
+@pytest.mark.parametrize("shape", range(6))
+@pytest.mark.parametrize("dims", [(5, 7, 2), (13, 3, 4), (41, 70, 9), (70, 9, 41), (24, 12, 13)])
+def test_fp32_operator_shapes(P, dims, shape):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=nx + ny, lo=0.05)
+    u = np.random.default_rng(2).normal(size=fmask.size)
+    u32 = u.astype(np.float32).astype(float)
+    y_ref = _oracle_apply(rho, KE, 3.0, nx, ny, nz, fmask, u32)
+    s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", fine_operator=3 + shape)
+    s.set_density(to_flat(rho), 3.0)
+    assert s.stats()["fine_form_fp32"] == 1 + shape
+    y = s.apply(torch.as_tensor(u, dtype=torch.float32).cuda()).double().cpu().numpy()
+    np.testing.assert_allclose(y, y_ref, rtol=0, atol=2e-6 * np.abs(y_ref).max())
+    ndof = fmask.size
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, ndof)).cuda()
+    U = s.solve(F)
+    r64 = HexSolver(nx, ny, nz, KE, fmask, precision="fp64", rtol=1e-12)
+    r64.set_density(to_flat(rho), 3.0)
+    U64 = r64.solve(F)
+    c, c64 = float(F @ U), float(F @ U64)
+    assert abs(c - c64) <= 1e-6 * abs(c64)
+    assert s.stats()["fp64_fallback"] == 0
+    s.close()
+    r64.close()
+
+
 @pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
 def test_fp64_solve_matches_reference_direct_solve(P, golden, tag):
     from pytopo3d_b200._tensors import to_flat
