@@ -342,6 +342,58 @@ int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int launches, do
  * written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
+/* ---------------------------------------------------------------------------
+ * A projection stage of the SIMP loop as one CUDA graph
+ * ------------------------------------------------------------------------- */
+
+/* The loop body of top3d (pytopo3d/core/optimizer.py:578-696: moduli, solves,
+ * sensitivities, OC update, change, re-projection) captured once per projection
+ * stage into the body of a device-side WHILE loop whose condition is decided on
+ * the device: continue while change > tolx and the stage's iteration limit is
+ * not reached (optimizer.py:578).  Each solve's CG loop is a nested WHILE node
+ * (the FP64 form's restart loop one more).  One launch runs the stage; the host
+ * reads the per-iteration record once.  Where the host path would have decided
+ * differently inside a solve (the mixed form's FP64 fallback, an FP64 solve the
+ * host path reports as failed) the pass raises counters[1], skips the rest of
+ * the iteration and ends the loop, with each case's warm-started initial guess
+ * in U_bak: the caller runs that iteration on the host path from U_bak (without
+ * a new set-up) and launches the graph again.
+ * All arrays are device arrays the caller owns and keeps at the same addresses
+ * for the graph's life; x is updated in place (x_new is the OC output).
+ * counters (5 ints, written by the caller before each launch): [0] iteration of
+ * the launch (0), [1] abort flag (0), [2] CG iterations of the running
+ * iteration (0), [3] iteration limit of the launch, [4] solves of the loop done
+ * before the launch (the warm start's history test).  record: limit x 8
+ * doubles per iteration: compliance, lambda, projected free volume, bisection
+ * steps, change, CG iterations, lambda bracket (lo, hi).  The solver must have
+ * run one loop body (set_density and a solve) on the host path before capture.
+ * No reference counterpart beyond the loop body itself. */
+typedef struct tp3d_stage tp3d_stage;
+typedef struct tp3d_stage_desc {
+  int ncases;                 /* load cases; F, U, U_prev, U_bak are ncases x ndof */
+  double rmin, beta, eta, penal, move, target_free_volume, tolx;
+  int max_bisection;
+  double bisection_tol;
+  const double* F;
+  double *U, *U_prev, *U_bak;
+  double *x, *x_new, *rho_f, *rho_p, *dproj, *rho_new;
+  double *dc_dx, *dc_acc, *dv_dx, *ce;
+  double* c;                  /* 2 doubles: compliance (and a case's share) */
+  const double* Hs;
+  const uint8_t *solid, *void_, *free_mask;
+  const double* KE_host;      /* 24x24 row-major, host */
+  void *sens_scratch, *oc_scratch;
+  double* oc_stats;           /* 8 doubles (tp3d_oc_update's stats) */
+  double* record;
+  int* counters;
+} tp3d_stage_desc;
+int tp3d_stage_capture(tp3d_solver* s, const tp3d_stage_desc* d, void* stream, tp3d_stage** out);
+/* Launch on `stream`, wait, and return the iterations completed and the abort flag. */
+int tp3d_stage_run(tp3d_stage* g, void* stream, int* iterations, int* aborted);
+/* Add a run's kernel launches (passes of the loop body, CG iterations) to tp3d_launch_count. */
+int tp3d_stage_count_launches(tp3d_stage* g, long long passes, long long cg_iterations);
+int tp3d_stage_destroy(tp3d_stage* g);
+
 /* Initial guess for the next solve of a load case from its last two solutions:
  * U <- 2 U - U_prev and U_prev <- (old) U; with have_prev == 0 only U_prev <- U.
  * Device arrays of n doubles.  The reference solves from scratch every

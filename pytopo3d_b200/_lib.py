@@ -63,6 +63,29 @@ class SolverOpts(C.Structure):
     ]
 
 
+class StageDesc(C.Structure):
+    """``tp3d_stage_desc`` of include/topo3d_b200.h."""
+
+    _fields_ = [
+        ("ncases", i32),
+        ("rmin", f64), ("beta", f64), ("eta", f64), ("penal", f64), ("move", f64),
+        ("target_free_volume", f64), ("tolx", f64),
+        ("max_bisection", i32),
+        ("bisection_tol", f64),
+        ("F", vp), ("U", vp), ("U_prev", vp), ("U_bak", vp),
+        ("x", vp), ("x_new", vp), ("rho_f", vp), ("rho_p", vp), ("dproj", vp), ("rho_new", vp),
+        ("dc_dx", vp), ("dc_acc", vp), ("dv_dx", vp), ("ce", vp),
+        ("c", vp),
+        ("Hs", vp),
+        ("solid", vp), ("void_", vp), ("free_mask", vp),
+        ("KE_host", vp),
+        ("sens_scratch", vp), ("oc_scratch", vp),
+        ("oc_stats", vp),
+        ("record", vp),
+        ("counters", vp),
+    ]
+
+
 # name -> (restype, argtypes); must match include/topo3d_b200.h
 SIGNATURES = {
     "tp3d_last_error": (C.c_char_p, []),
@@ -97,6 +120,10 @@ SIGNATURES = {
     "tp3d_solver_time_level": (i32, [vp, i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),
     "tp3d_solver_stats": (i32, [vp, C.POINTER(f64), i32]),
     "tp3d_warm_start": (i32, [vp, vp, i64, i32, vp]),
+    "tp3d_stage_capture": (i32, [vp, C.POINTER(StageDesc), vp, C.POINTER(vp)]),
+    "tp3d_stage_run": (i32, [vp, vp, C.POINTER(i32), C.POINTER(i32)]),
+    "tp3d_stage_count_launches": (i32, [vp, i64, i64]),
+    "tp3d_stage_destroy": (i32, [vp]),
 }
 
 _lib = None

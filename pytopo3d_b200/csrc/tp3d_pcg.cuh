@@ -228,3 +228,138 @@ __global__ void scale_copy_kernel(long long n, const T* __restrict__ src, const 
 }
 
 }  // namespace tp3d
+
+namespace tp3d {
+
+// ---------------------------------------------------------------------------
+// Kernels of the captured SIMP stage (one CUDA graph per projection stage):
+// every host decision of the loop body becomes a device value.
+// ---------------------------------------------------------------------------
+
+// Stage counters (device ints): iteration of the launch, abort flag, CG
+// iterations of the running iteration, iteration limit of the launch, solves
+// done before the launch.
+enum StageCounter : int { kStIter = 0, kStAbort, kStCg, kStLimit, kStBase, kStCount };
+constexpr int kStageRecord = 8;  // doubles per recorded iteration
+
+// A conditional node's value is assigned its default only when the graph is
+// launched: a WHILE node nested in another loop's body is re-armed by this
+// kernel before each entry.
+__global__ void arm_conditional_kernel(cudaGraphConditionalHandle h) { cudaGraphSetConditional(h, 1u); }
+
+// The solver state of a new solve, as the host path writes it before a solve.
+__global__ void init_state_kernel(PcgState* st, int max_iters, double delta2) {
+  PcgState z{};
+  z.max_iters = max_iters;
+  z.delta2 = delta2;
+  *st = z;
+}
+
+// Extrapolated initial guess (warm_start_kernel) with the history test on the
+// device: the last two solutions exist once base + iteration >= 2 solves were done.
+__global__ void warm_start_dev_kernel(long long n, double* U, double* U_prev, const int* ctr) {
+  const int have_prev = ctr[kStBase] + ctr[kStIter] >= 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double u = U[i];
+    if (have_prev) U[i] = 2.0 * u - U_prev[i];
+    U_prev[i] = u;
+  }
+}
+
+// After a queued mixed solve: whether the host path would have accepted it
+// without its FP64 fallback (converged, or at its residual floor).  Otherwise
+// *abort is raised.  The solve's CG iterations are summed into *cg.
+__global__ void solve_status_kernel(const PcgState* st, int* abort, int* cg) {
+  const PcgState s = *st;
+  if (!(s.done == 1 || s.done == 5)) *abort = 1;
+  *cg += s.iters;
+}
+
+// Restart state of an FP64 solve queued in a stage graph (the host path's
+// solve64 loop): [0] residual of the previous run, [1] CG iterations so far,
+// [2] restarts so far.
+__global__ void restart_init_kernel(double* rs) {
+  rs[0] = INFINITY;
+  rs[1] = 0.0;
+  rs[2] = 0.0;
+}
+
+// The solver state of the next run of that loop: the iteration budget left.
+__global__ void init_state_budget_kernel(PcgState* st, const double* rs, int max_iters) {
+  PcgState z{};
+  z.max_iters = max(1, max_iters - (int)rs[1]);
+  *st = z;
+}
+
+// After a run and its true residual (st->rr = ||f - K u||^2): the decisions of
+// the host path's solve64, taken on the device.  Accept (relative residual
+// within 2 rtol, or the residual floor: a converged run whose restart no
+// longer halved it), restart (set the loop condition), or hand the solve back
+// to the host (breakdown, non-finite, not converged within the budget).
+__global__ void restart_decide_kernel(cudaGraphConditionalHandle h, const PcgState* st, double* rs, double rtol,
+                                      int max_restarts, int max_iters, int* abort, int* cg) {
+  const PcgState s = *st;
+  const double total = rs[1] + s.iters;
+  rs[1] = total;
+  *cg += s.iters;
+  bool again = false;
+  if (s.done == 3 || s.done == 4 || s.done == 7) {
+    *abort = 1;
+  } else if (s.bb != 0.0) {
+    const bool run_ok = s.done == 1 || s.done == 5;
+    const double relres = sqrt(fmax(s.rr, 0.0) / s.bb);
+    if (!isfinite(relres)) {
+      *abort = 1;
+    } else if (relres <= 2.0 * rtol) {
+      // accepted
+    } else if (run_ok && relres > 0.5 * rs[0]) {
+      // residual floor: accepted
+    } else if (!run_ok || rs[2] >= max_restarts || total >= max_iters) {
+      *abort = 1;
+    } else {
+      rs[0] = relres;
+      rs[2] += 1.0;
+      again = true;
+    }
+  }
+  cudaGraphSetConditional(h, again ? 1u : 0u);
+}
+
+// Several load cases: dc += dc_case, c[0] += c[1] (the host path's sums).
+__global__ void accumulate_case_kernel(long long n, double* dc, const double* __restrict__ dc_case, double* c) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dc[i] += dc_case[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) c[0] += c[1];
+}
+
+// Gate of the iteration's second half (sensitivities, OC, projection).
+__global__ void stage_gate_kernel(cudaGraphConditionalHandle h, const int* ctr) {
+  cudaGraphSetConditional(h, ctr[kStAbort] == 0 ? 1u : 0u);
+}
+
+// End of an iteration: record [c, lambda, volume, steps, change, CG
+// iterations, lambda bracket] at the iteration's slot, advance the counter and
+// decide the stage loop (change > tolx and below the limit, no abort).
+__global__ void stage_next_kernel(cudaGraphConditionalHandle h, int* ctr, const double* __restrict__ c,
+                                  const double* __restrict__ oc, double* record, double tolx) {
+  if (ctr[kStAbort]) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  const int it = ctr[kStIter];
+  double* r = record + (size_t)it * kStageRecord;
+  r[0] = c[0];
+  r[1] = oc[0];
+  r[2] = oc[1];
+  r[3] = oc[2];
+  r[4] = oc[3];
+  r[5] = (double)ctr[kStCg];
+  r[6] = oc[5];
+  r[7] = oc[6];
+  ctr[kStIter] = it + 1;
+  ctr[kStCg] = 0;
+  const bool go = oc[3] > tolx && it + 1 < ctr[kStLimit];
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+}  // namespace tp3d

@@ -351,6 +351,8 @@ struct tp3d_solver {
     if (state_host) cudaFreeHost(state_host);
     if (loop_pass_host) cudaFreeHost(loop_pass_host);
     if (st_branch) cudaStreamDestroy(st_branch);
+    if (st_loop) cudaStreamDestroy(st_loop);
+    if (st_restart) cudaStreamDestroy(st_restart);
     if (st_side) cudaStreamDestroy(st_side);
     for (cudaStream_t p : st_pow) if (p) cudaStreamDestroy(p);
     for (cudaEvent_t e : ev_pow_in) if (e) cudaEventDestroy(e);
@@ -1228,6 +1230,152 @@ struct tp3d_solver {
       return TP3D_ERR_TIMEOUT;
     }
     return TP3D_NOT_CONVERGED;
+  }
+
+  // ---------------- solves inside a captured SIMP stage ----------------
+  cudaStream_t st_loop = nullptr, st_restart = nullptr;
+  long long stage_loop_kernels = 0;  // kernels of one CG iteration in the last loop captured this way
+  double* restart_state = nullptr;   // device [previous residual, iterations, restarts] (stage graphs)
+
+  // A WHILE node added to the graph that `st` is being captured into; its body
+  // is captured by body(handle) on `other` (swapped in as `st` meanwhile) and
+  // must end with a kernel that sets the handle's condition.  The node is
+  // re-armed by a kernel before it (a nested loop runs once per entry).
+  template <class Body>
+  int while_into(cudaStream_t& other, Body body) {
+    if (!other) return TP3D_ERR_ARG;  // created before the capture
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle hw = 0;
+    TP3D_CHECK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) {
+      tp3d_set_last_error("while_into: the solver stream is not capturing");
+      return TP3D_ERR_ARG;
+    }
+    TP3D_CHECK(cudaGraphConditionalHandleCreate(&hw, capg, 1, cudaGraphCondAssignDefault));
+    arm_conditional_kernel<<<1, 1, 0, st>>>(hw);
+    TP3D_CHECK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hw;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    TP3D_CHECK(cudaGraphAddNode(&wnode, capg, deps, nd, &cp));
+    TP3D_CHECK(cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies));
+    std::swap(st, other);
+    int rc = TP3D_OK;
+    if (cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      rc = TP3D_ERR_CUDA;
+    } else {
+      plain_next = true;
+      rc = body(hw);
+      cudaGraph_t out = nullptr;
+      if (cudaStreamEndCapture(st, &out) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    }
+    std::swap(st, other);
+    plain_next = true;
+    return rc;
+  }
+
+  // The CG iteration as a WHILE node in the graph being captured (the caller's
+  // stage graph); the reliable-update branch inside becomes a nested IF node as
+  // in capture_loop.  Nothing is instantiated here: the stage graph holds the loop.
+  template <class Body>
+  int capture_loop_into(Body body) {
+    TP3D_CHECK(cudaMemsetAsync(loop_passes, 0, sizeof(unsigned int), st));
+    long long* outer = t_capture_count;
+    t_capture_count = &stage_loop_kernels;
+    stage_loop_kernels = 0;
+    const int rc = while_into(st_loop, [&](cudaGraphConditionalHandle hw) {
+      in_loop_capture = true;
+      branch_ok = true;
+      pdl_region = true;
+      plain_next = true;
+      int r = body();
+      pdl_region = false;
+      set_loop_cond_kernel<<<1, 1, 0, st>>>(hw, state, loop_passes, (unsigned int)o.max_iterations + 16u);
+      ++stage_loop_kernels;
+      in_loop_capture = false;
+      if (!branch_ok) r = TP3D_ERR_CUDA;
+      return r;
+    });
+    t_capture_count = outer;
+    if (rc) tp3d_set_last_error("capture of the CG loop into the stage graph failed");
+    return rc;
+  }
+
+  // One solve of K U = F queued on the caller's (capturing) stream with no host
+  // synchronisation: the host path's prologue (its state written by a kernel),
+  // the CG loop as a WHILE node and the FP64 result.  The mixed form raises
+  // *abort when the host path would have finished the solve with its FP64
+  // fallback; the FP64 form runs the host path's restart loop (run, true
+  // residual, restart) as a WHILE node and raises *abort where the host path
+  // would have reported a failure.  *cg accumulates the CG iterations.
+  int solve_into_capture(const double* F, double* U, int* abort, int* cg) {
+    const long long nn = g.nnode(), ndof = 3 * nn;
+    const int nb = grid_blocks(ndof);
+    if (int e = enter()) return e;
+    if (cyc_bar) TP3D_CHECK(cudaMemsetAsync(cyc_bar, 0, 2 * sizeof(unsigned int), st));
+    TP3D_CHECK(cudaMemcpyAsync(u64, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    zero_fixed_kernel<<<grid_blocks(nn), 256, 0, st>>>(nn, u64, fix[0]);
+    int rc = TP3D_OK;
+    if (mixed) {
+      init_state_kernel<<<1, 1, 0, st>>>(state, o.max_iterations, o.reliable_delta * o.reliable_delta);
+      TP3D_CHECK(cudaMemcpyAsync(F_capture, F, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      masked_norm_kernel<<<grid_blocks(nn), 256, 0, st>>>(nn, F, fix[0], partials);
+      finalize_kernel<<<1, 256, 0, st>>>(partials, grid_blocks(nn), state, kFinBB, o.rtol * o.rtol, nullptr);
+      OpIO<double> r;
+      r.u = u64;
+      r.out = r64;
+      r.b = F;
+      rc |= fine<double, kModeResid>(r);
+      dot_kernel<double><<<nb, 256, 0, st>>>(ndof, r64, r64, partials, nullptr, nullptr);
+      finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRInit, 0.0, nullptr);
+      demote_kernel<<<nb, 256, 0, st>>>(ndof, r64, K32.r, state, 1);
+      TP3D_CHECK(cudaMemsetAsync(K32.u, 0, ndof * sizeof(float), st));
+      float* z = vcycle<float>(0, K32.r, &state->done, &rc);
+      dot_kernel<float><<<nb, 256, 0, st>>>(ndof, K32.r, z, partials, &state->done, nullptr);
+      finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZInit, 0.0, nullptr);
+      cg_p_kernel<float><<<nb, 256, 0, st>>>(ndof, z, K32.p, state, 1);
+      if (rc == TP3D_OK) rc = capture_loop_into([&]() { return mixed_iteration(); });
+      flush_kernel<<<nb, 256, 0, st>>>(ndof, u64, K32.u, state, 1);
+      solve_status_kernel<<<1, 1, 0, st>>>(state, abort, cg);
+    } else {
+      if (!restart_state) return TP3D_ERR_ARG;  // allocated before the capture (tp3d_stage_capture)
+      restart_init_kernel<<<1, 1, 0, st>>>(restart_state);
+      if (rc == TP3D_OK)
+        rc = while_into(st_restart, [&](cudaGraphConditionalHandle hr) {
+          int r = TP3D_OK;
+          init_state_budget_kernel<<<1, 1, 0, st>>>(state, restart_state, o.max_iterations);
+          masked_norm_kernel<<<grid_blocks(nn), 256, 0, st>>>(nn, F, fix[0], partials);
+          finalize_kernel<<<1, 256, 0, st>>>(partials, grid_blocks(nn), state, kFinBB, o.rtol * o.rtol, nullptr);
+          OpIO<double> io;
+          io.u = K64.u;
+          io.out = K64.r;
+          io.b = F;
+          r |= fine<double, kModeResid>(io);
+          dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K64.r, K64.r, partials, nullptr, nullptr);
+          finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRRInit, 0.0, nullptr);
+          double* z = vcycle<double>(0, K64.r, &state->done, &r);
+          dot_kernel<double><<<nb, 256, 0, st>>>(ndof, K64.r, z, partials, &state->done, nullptr);
+          finalize_kernel<<<1, 256, 0, st>>>(partials, nb, state, kFinRZInit, 0.0, nullptr);
+          cg_p_kernel<double><<<nb, 256, 0, st>>>(ndof, z, K64.p, state, 1);
+          if (r == TP3D_OK) r = capture_loop_into([&]() { return pcg64_iteration(); });
+          // the true residual, into state->rr where the host path's check reads it
+          if (r == TP3D_OK) r = true_residual(F, K64.u, K64.q, &state->rr);
+          restart_decide_kernel<<<1, 1, 0, st>>>(hr, state, restart_state, o.rtol, o.max_restarts,
+                                                 o.max_iterations, abort, cg);
+          return r;
+        });
+    }
+    TP3D_CHECK(cudaMemcpyAsync(U, u64, ndof * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    TP3D_CHECK_LAUNCH();
+    if (rc) return rc;
+    return leave();
   }
 
   // ---------------- FP64 PCG ----------------
@@ -2382,4 +2530,223 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;
+}
+
+// ---------------------------------------------------------------------------
+// A projection stage of the SIMP loop as one CUDA graph.
+//
+// The loop body of pytopo3d/core/optimizer.py:578-696 (warm start, moduli and
+// multigrid set-up, the solves, sensitivities, OC bisection, re-projection) is
+// captured once per stage into the body of a WHILE node whose condition a
+// kernel sets at the end of every pass: change > tolx and the stage's
+// iteration limit not reached (optimizer.py:578).  Each solve's CG loop is a
+// nested WHILE node (the FP64 form's restart loop one more).  One launch runs
+// the stage; the host reads the per-iteration record once.  Where the host
+// path would have decided differently inside a solve (the mixed form's FP64
+// fallback; an FP64 solve the host path reports as failed) the pass raises the
+// abort flag: the rest of the iteration is skipped (an IF node), the
+// warm-started initial guesses are kept in U_bak, the loop ends, and the
+// caller runs that iteration on the host path before launching again.
+// ---------------------------------------------------------------------------
+struct tp3d_stage {
+  cudaGraphExec_t exec = nullptr;
+  tp3d_solver* s = nullptr;
+  int* counters = nullptr;
+  long long body_kernels = 0, loop_kernels = 0;
+};
+
+namespace {
+
+// Adds a conditional IF node on handle h after the work captured so far on
+// `cs` and starts capturing its body on `body_st`.
+int begin_if_body(cudaStream_t cs, cudaStream_t body_st, cudaGraphConditionalHandle h) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t capg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  TP3D_CHECK(cudaStreamGetCaptureInfo(cs, &st, nullptr, &capg, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  TP3D_CHECK(cudaGraphAddNode(&node, capg, deps, nd, &cp));
+  TP3D_CHECK(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  TP3D_CHECK(cudaStreamBeginCaptureToGraph(body_st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+  return TP3D_OK;
+}
+
+int stage_body(tp3d_solver* s, const tp3d_stage_desc* d, cudaStream_t cs, cudaStream_t cs2,
+               cudaGraphConditionalHandle h_stage, long long* body_kernels) {
+  const Grid& g = s->g;
+  const long long ndof = 3 * g.nnode(), nele = g.nele();
+  const int nb = s->grid_blocks(ndof);
+  int* ctr = d->counters;
+  for (int k = 0; k < d->ncases; ++k) {
+    double* U = d->U + (size_t)k * ndof;
+    warm_start_dev_kernel<<<nb, 256, 0, cs>>>(ndof, U, d->U_prev + (size_t)k * ndof, ctr);
+    TP3D_CHECK(cudaMemcpyAsync(d->U_bak + (size_t)k * ndof, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+  }
+  *body_kernels += d->ncases;
+  if (int rc = tp3d_solver_set_density(s, d->rho_p, d->penal)) return rc;
+  for (int k = 0; k < d->ncases; ++k)
+    if (int rc = s->solve_into_capture(d->F + (size_t)k * ndof, d->U + (size_t)k * ndof, ctr + kStAbort,
+                                       ctr + kStCg))
+      return rc;
+  // the iteration's second half, skipped when a solve raised the abort flag
+  cudaGraphConditionalHandle hg = 0;
+  {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t capg = nullptr;
+    TP3D_CHECK(cudaStreamGetCaptureInfo(cs, &st, nullptr, &capg, nullptr, nullptr));
+    TP3D_CHECK(cudaGraphConditionalHandleCreate(&hg, capg, 0, cudaGraphCondAssignDefault));
+  }
+  stage_gate_kernel<<<1, 1, 0, cs>>>(hg, ctr);
+  if (int rc = begin_if_body(cs, cs2, hg)) return rc;
+  int rc = TP3D_OK;
+  for (int k = 0; k < d->ncases && rc == TP3D_OK; ++k) {
+    rc = tp3d_sensitivity(g.nx, g.ny, g.nz, d->rmin, d->U + (size_t)k * ndof, d->KE_host, d->rho_p, d->dproj,
+                          d->Hs, d->free_mask, d->penal, d->ce, k == 0 ? d->dc_dx : d->dc_acc, d->dv_dx,
+                          d->c + std::min(k, 1), d->sens_scratch, cs2);
+    if (rc == TP3D_OK && k > 0) {
+      accumulate_case_kernel<<<s->grid_blocks(nele), 256, 0, cs2>>>(nele, d->dc_dx, d->dc_acc, d->c);
+      ++*body_kernels;
+    }
+  }
+  if (rc == TP3D_OK)
+    rc = tp3d_oc_update(g.nx, g.ny, g.nz, d->rmin, d->x, d->dc_dx, d->dv_dx, d->Hs, d->solid, d->void_, d->move,
+                        d->target_free_volume, d->beta, d->eta, d->max_bisection, d->bisection_tol, d->x_new,
+                        d->rho_new, d->oc_stats, d->oc_scratch, cs2);
+  if (rc == TP3D_OK &&
+      cudaMemcpyAsync(d->x, d->x_new, nele * sizeof(double), cudaMemcpyDeviceToDevice, cs2) != cudaSuccess)
+    rc = TP3D_ERR_CUDA;
+  if (rc == TP3D_OK)
+    rc = tp3d_filter_project(g.nx, g.ny, g.nz, d->rmin, d->x, d->Hs, d->beta, d->eta, d->solid, d->void_, d->rho_f,
+                             d->rho_p, d->dproj, cs2);
+  cudaGraph_t out = nullptr;
+  if (cudaStreamEndCapture(cs2, &out) != cudaSuccess && rc == TP3D_OK) rc = TP3D_ERR_CUDA;
+  if (rc) return rc;
+  stage_next_kernel<<<1, 1, 0, cs>>>(h_stage, ctr, d->c, d->oc_stats, d->record, d->tolx);
+  *body_kernels += 4 + 2 * d->ncases;  // gate, next, OC, projection, sensitivity launches
+  TP3D_CHECK_LAUNCH();
+  return TP3D_OK;
+}
+
+}  // namespace
+
+extern "C" int tp3d_stage_capture(tp3d_solver* s, const tp3d_stage_desc* d, void* stream, tp3d_stage** out) {
+  if (!s || !d || !out || d->ncases < 1 || !d->F || !d->U || !d->U_prev || !d->U_bak || !d->x || !d->x_new ||
+      !d->rho_f || !d->rho_p || !d->dproj || !d->rho_new || !d->dc_dx || !d->dv_dx || !d->ce || !d->c || !d->Hs ||
+      !d->free_mask || !d->KE_host || !d->sens_scratch || !d->oc_scratch || !d->oc_stats || !d->record ||
+      !d->counters || (d->ncases > 1 && !d->dc_acc))
+    return TP3D_ERR_ARG;
+  if (!s->have_density || !s->fine_chosen || s->pending) {
+    tp3d_set_last_error("tp3d_stage_capture: run one loop body on the host path first");
+    return TP3D_ERR_ARG;
+  }
+  (void)stream;
+  *out = nullptr;
+  // what the capture needs but may not create while capturing: streams, the
+  // restart state, and the mixed form's FP64 fallback hierarchy (so that the
+  // captured set-up refreshes it exactly as the host path's does)
+  if (!s->restart_state) s->restart_state = s->alloc<double>(4);
+  if (!s->restart_state) return TP3D_ERR_CUDA;
+  if (!s->st_loop) TP3D_CHECK(cudaStreamCreateWithFlags(&s->st_loop, cudaStreamNonBlocking));
+  if (!s->st_restart) TP3D_CHECK(cudaStreamCreateWithFlags(&s->st_restart, cudaStreamNonBlocking));
+  if (s->mixed) {
+    if (int e = s->enter()) return e;
+    if (int e = s->ensure_fp64_buffers()) return e;
+    if (int e = s->leave()) return e;
+  }
+  cudaStream_t cs = nullptr, cs2 = nullptr;
+  TP3D_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  TP3D_CHECK(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking));
+  TP3D_CHECK(cudaDeviceSynchronize());
+  auto* gph = new tp3d_stage();
+  gph->s = s;
+  gph->counters = d->counters;
+  int rc = TP3D_OK;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    cudaGraph_t G = nullptr;
+    cudaGraphConditionalHandle hs = 0;
+    rc = TP3D_OK;
+    if (cudaGraphCreate(&G, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&hs, G, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+      rc = TP3D_ERR_CUDA;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t wnode;
+    if (rc == TP3D_OK) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = hs;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      if (cudaGraphAddNode(&wnode, G, nullptr, 0, &cp) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    }
+    bool capturing = false;
+    cudaStream_t saved_user = s->user;
+    if (rc == TP3D_OK) {
+      capturing = cudaStreamBeginCaptureToGraph(cs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (!capturing) rc = TP3D_ERR_CUDA;
+    }
+    if (rc == TP3D_OK) {
+      s->user = cs;
+      long long nk = 0;
+      t_capture_count = &nk;
+      rc = stage_body(s, d, cs, cs2, hs, &gph->body_kernels);
+      t_capture_count = nullptr;
+      gph->body_kernels += nk;
+      gph->loop_kernels = s->stage_loop_kernels;
+      s->user = saved_user;
+    }
+    if (capturing) {
+      cudaGraph_t o2 = nullptr;
+      if (cudaStreamEndCapture(cs, &o2) != cudaSuccess && rc == TP3D_OK) rc = TP3D_ERR_CUDA;
+    }
+    if (rc == TP3D_OK && cudaGraphInstantiate(&gph->exec, G, 0) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    if (G) cudaGraphDestroy(G);
+    cudaGetLastError();
+    if (rc == TP3D_OK) break;
+    if (gph->exec) cudaGraphExecDestroy(gph->exec);
+    gph->exec = nullptr;
+    gph->body_kernels = 0;
+    if (!s->pdl) break;
+    s->pdl = false;  // retry in plain stream order
+  }
+  cudaStreamDestroy(cs);
+  cudaStreamDestroy(cs2);
+  if (rc) {
+    delete gph;
+    if (!*tp3d_last_error()) tp3d_set_last_error("stage graph capture failed");
+    return rc;
+  }
+  *out = gph;
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_stage_run(tp3d_stage* g, void* stream, int* iterations, int* aborted) {
+  if (!g || !g->exec) return TP3D_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  TP3D_CHECK(cudaGraphLaunch(g->exec, st));
+  int c[kStCount] = {};
+  TP3D_CHECK(cudaMemcpyAsync(c, g->counters, sizeof(c), cudaMemcpyDeviceToHost, st));
+  TP3D_CHECK(cudaStreamSynchronize(st));
+  if (iterations) *iterations = c[kStIter];
+  if (aborted) *aborted = c[kStAbort];
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_stage_count_launches(tp3d_stage* g, long long passes, long long cg_iterations) {
+  if (!g) return TP3D_ERR_ARG;
+  add_launches(passes * g->body_kernels + cg_iterations * g->loop_kernels);
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_stage_destroy(tp3d_stage* g) {
+  if (!g) return TP3D_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  delete g;
+  return TP3D_OK;
 }

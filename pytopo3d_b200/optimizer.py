@@ -11,11 +11,15 @@ Extensions (keyword-only): ``F`` — an explicit nodal load vector, or a 2-D
 array of load cases whose compliances are summed; ``precision`` — "fp64"
 (default) or "mixed"; ``solver_options`` — HexSolver options;
 ``record`` — a list receiving per-iteration stats (and the iteration's new
-design as a flat device tensor, key ``x``).
+design as a flat device tensor, key ``x``, for iterations run on the host
+path); ``stage_graph`` — run each projection stage's loop bodies as one CUDA
+graph launch, the stage's loop condition decided on the device
+(``StageGraph``; not with ``save_history``).
 """
 
 from __future__ import annotations
 
+import ctypes as C
 import logging
 import time
 from typing import Any, Dict, MutableMapping, Optional, Sequence, Tuple, Union
@@ -153,15 +157,20 @@ class SimpState:
         starts from the last solution, not from an extrapolation across the jump."""
         self.n_solved = min(self.n_solved, 1)
 
-    def sensitivities(self, rho_p, dproj):
-        """Solve every load case, then fused energy / compliance / chain rule."""
+    def sensitivities(self, rho_p, dproj, rerun=False):
+        """Solve every load case, then fused energy / compliance / chain rule.
+        ``rerun``: the iteration that a stage graph handed back after its set-up
+        and warm start, so U already holds the initial guesses and the solver
+        the hierarchy of rho_p."""
         L = _lib.lib()
         H = self.H
-        self.solver.set_density(rho_p, self.penal)
+        if not rerun:
+            self.solver.set_density(rho_p, self.penal)
         iters = 0
         for k in range(self.F.shape[0]):
-            _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
-                                         1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
+            if not rerun:
+                _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
+                                             1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
             dst_dc = self.dc_dx if k == 0 else self.dc_acc
             if k == 0 and self.solver.autotune_pending and self.n_iter + 1 >= self.solver.autotune_at:
                 self.solver.autotune(self.F[k], self.U[k])
@@ -187,6 +196,74 @@ class SimpState:
         self.n_solved += 1
         self.n_iter += 1
         return iters
+
+
+class StageGraph:
+    """One projection stage of the loop body as a CUDA graph (tp3d_stage_*).
+
+    Captured for the state ``S`` and the stage's projection parameters; ``x``
+    is updated in place (the host path must then copy, not swap, the new
+    design).  ``run(limit)`` launches it once: up to ``limit`` loop bodies,
+    ending early when change <= tolx; returns (records, aborted), a record per
+    completed iteration [c, lambda, volume, steps, change, CG iterations, lo,
+    hi].  After an abort, each case's warm-started initial guess is in
+    ``U_bak``: the caller reruns that iteration on the host path from there.
+    """
+
+    def __init__(self, S: "SimpState", x, beta, eta, move, target, tolx, capacity,
+                 max_bisection=80, bisection_tol=1e-8):
+        self.S = S
+        n = x.numel()
+        self.capacity = int(capacity)
+        self.counters = torch.zeros(8, dtype=torch.int32, device=device())
+        self.record = torch.zeros((self.capacity, 8), dtype=torch.float64, device=device())
+        self.U_bak = torch.empty_like(S.U)
+        self.rho_new = torch.empty(n, dtype=torch.float64, device=device())
+        d = _lib.StageDesc()
+        d.ncases = S.F.shape[0]
+        d.rmin, d.beta, d.eta, d.penal, d.move = float(S.H.rmin), float(beta), float(eta), S.penal, float(move)
+        d.target_free_volume, d.tolx = float(target), float(tolx)
+        d.max_bisection, d.bisection_tol = int(max_bisection), float(bisection_tol)
+        d.F, d.U, d.U_prev, d.U_bak = S.F.data_ptr(), S.U.data_ptr(), S.U_prev.data_ptr(), self.U_bak.data_ptr()
+        d.x, d.x_new = x.data_ptr(), S.x_new.data_ptr()
+        d.rho_f, d.rho_p, d.dproj, d.rho_new = (S.rho_f.data_ptr(), S.rho_p.data_ptr(), S.dproj.data_ptr(),
+                                                self.rho_new.data_ptr())
+        d.dc_dx, d.dc_acc, d.dv_dx, d.ce = S.dc_dx.data_ptr(), S.dc_acc.data_ptr(), S.dv_dx.data_ptr(), S.ce.data_ptr()
+        d.c = S.c_dev.data_ptr()
+        d.Hs = S.Hs.data_ptr()
+        d.solid, d.void_, d.free_mask = _lib.ptr(S.solid), _lib.ptr(S.void), S.free.data_ptr()
+        d.KE_host = S.KE.ctypes.data
+        d.sens_scratch, d.oc_scratch = S.sens_scratch.data_ptr(), S.ws.scratch.data_ptr()
+        d.oc_stats = S.ws.stats.data_ptr()
+        d.record, d.counters = self.record.data_ptr(), self.counters.data_ptr()
+        self._desc = d
+        self._x = x
+        h = C.c_void_p()
+        _lib.check(_lib.lib().tp3d_stage_capture(S.solver._h, C.byref(d), _lib.stream_ptr(), C.byref(h)),
+                   "stage_capture")
+        self._h = h
+
+    def run(self, limit: int):
+        limit = min(int(limit), self.capacity)
+        self.counters.copy_(torch.tensor([0, 0, 0, limit, self.S.n_solved, 0, 0, 0], dtype=torch.int32))
+        it, ab = C.c_int(0), C.c_int(0)
+        _lib.check(_lib.lib().tp3d_stage_run(self._h, _lib.stream_ptr(), C.byref(it), C.byref(ab)), "stage_run")
+        rec = self.record[:it.value].cpu().numpy().copy()
+        _lib.lib().tp3d_stage_count_launches(self._h, it.value + ab.value, int(rec[:, 5].sum()) if len(rec) else 0)
+        self.S.n_solved += it.value
+        self.S.n_iter += it.value
+        return rec, bool(ab.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().tp3d_stage_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class SimpLoop:
@@ -310,6 +387,7 @@ def top3d(
     precision: str = "fp64",
     solver_options: Optional[Dict[str, Any]] = None,
     record: Optional[list] = None,
+    stage_graph: bool = False,
 ) -> Tuple[np.ndarray, Optional[Dict[str, list]], float, None]:
     """Density-filtered SIMP with Heaviside continuation (optimizer.py:283-839).
 
@@ -383,6 +461,10 @@ def top3d(
             out.append(float(rp[free.bool()].mean()))
         return out
 
+    # one CUDA graph launch per projection stage (after the run's first loop body,
+    # which sets the solver up); per-iteration densities are not kept on the
+    # device, so a run that saves its history stays on the host path
+    use_graph = bool(stage_graph) and not save_history
     total_loop = 0
     c = float("nan")
     snap = torch.empty(nelx * nely * nelz, dtype=torch.float64, pin_memory=True) if save_history else None
@@ -404,7 +486,42 @@ def top3d(
             logger.warning("Projected free-volume target %.6f exceeds the maximum achievable %.6f at "
                            "beta=%g; the volume upper bound is inactive at the all-solid free design.",
                            volfrac, vmax, beta)
+        graph = None
+        rerun = False  # the next host iteration reruns one that the stage graph handed back
         while change > tolx and stage_loop < maxloop:
+            if use_graph and not rerun and not solver.autotune_pending and total_loop > 0:
+                # the rest of the stage as one graph launch (until change <= tolx,
+                # maxloop, or a solve that the host path has to finish)
+                if graph is None:
+                    try:
+                        graph = StageGraph(S, x, beta, projection_eta, move, target_free_volume, tolx, maxloop)
+                    except _lib.Topo3dError as e:
+                        logger.warning("stage graph unavailable (%s); the loop runs on the host path", e)
+                        use_graph = False
+                        continue
+                t0 = time.time()
+                rec_arr, aborted = graph.run(maxloop - stage_loop)
+                dt = (time.time() - t0) / max(1, len(rec_arr))
+                for r in rec_arr:
+                    stage_loop += 1
+                    total_loop += 1
+                    c, change = float(r[0]), float(r[4])
+                    if not np.isfinite(r[3]):
+                        raise _lib.Topo3dError("OC bisection did not finish (bounded device wait expired)")
+                    c_delta = c - c_prev if np.isfinite(c_prev) else float("nan")
+                    c_prev = c
+                    if record is not None:
+                        record.append(dict(beta=beta, c=c, change=change, cg_iterations=int(r[5]),
+                                           relres=float("nan"), bisection_steps=int(r[3]), lam=float(r[1]),
+                                           stage_graph=True))
+                    logger.info("beta=%4.1f iter=%4d total=%4d C=%.6e dC=%.3e change=%.5e time=%.4fs cg=%d "
+                                "(stage graph)", beta, stage_loop, total_loop, c, c_delta, change, dt, int(r[5]))
+                if aborted:
+                    # a solve that the host path finishes differently: rerun that
+                    # iteration from its warm-started initial guesses
+                    S.U.copy_(graph.U_bak)
+                    rerun = True
+                continue
             stage_loop += 1
             total_loop += 1
             t0 = time.time()
@@ -412,14 +529,18 @@ def top3d(
                 # the design this iteration solves on, copied to pinned host memory
                 # while the iteration runs (read only if the iteration is recorded)
                 snap.copy_(S.rho_p, non_blocking=True)
-            cg_iters = S.sensitivities(S.rho_p, S.dproj)
+            cg_iters = S.sensitivities(S.rho_p, S.dproj, rerun=rerun)
+            rerun = False
             stats = oc_update_flat(H, x, S.dc_dx, S.dv_dx, Hs, solid, void, move, target_free_volume, beta,
                                    projection_eta, S.x_new, S.rho_new, S.ws)
             host = torch.cat([S.c_dev[:1], stats]).cpu().numpy()
             c, change = float(host[0]), float(host[4])
             if not np.isfinite(host[3]):
                 raise _lib.Topo3dError("OC bisection did not finish (bounded device wait expired)")
-            x, S.x_new = S.x_new, x
+            if use_graph:
+                x.copy_(S.x_new)  # the stage graph holds x's address
+            else:
+                x, S.x_new = S.x_new, x
             c_delta = c - c_prev if np.isfinite(c_prev) else float("nan")
             c_prev = c
             if record is not None:
@@ -438,6 +559,8 @@ def top3d(
                             "change=%.5e time=%.2fs cg=%d", beta, stage_loop, total_loop, c, c_delta, vol,
                             gray, change, time.time() - t0, cg_iters)
             S.project(x, beta, projection_eta)
+        if graph is not None:
+            graph.close()
         vol, gray = _free_stats(S.rho_p, free)
         converged = change <= tolx
         if not converged:

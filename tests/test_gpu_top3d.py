@@ -173,3 +173,30 @@ def test_mixed_precision_top3d_tracks_fp64(P):
     x32, _, c32, _ = P.top3d(**kw, record=r32, precision="mixed")
     assert abs(r32[0]["c"] - r64[0]["c"]) <= 1e-6 * abs(r64[0]["c"])
     assert abs(c32 - c64) <= 1e-5 * abs(c64)
+
+
+@pytest.mark.parametrize("precision,opts", [("fp64", {}), ("mixed", {}),
+                                            ("mixed", {"max_iterations": 12})])
+def test_stage_graph_matches_host_path(P, precision, opts):
+    """Each projection stage as one CUDA graph launch (the loop condition
+    decided on the device) reproduces the host-driven loop bit for bit.  With
+    an iteration cap of 12 the mixed solves stop short, the graph hands those
+    iterations back and the host path finishes them with its FP64 fallback."""
+    kw = dict(nelx=16, nely=8, nelz=8, volfrac=0.3, penal=3.0, rmin=1.5, disp_thres=0.5, elem_size=1.0,
+              tolx=0.01, maxloop=8, beta_schedule=(1.0, 2.0, 4.0), precision=precision, solver_options=opts)
+    r_host, r_graph, d_host, d_graph = [], [], {}, {}
+    x_host, _, c_host, _ = P.top3d(**kw, record=r_host, diagnostics_out=d_host)
+    x_graph, _, c_graph, _ = P.top3d(**kw, record=r_graph, diagnostics_out=d_graph, stage_graph=True)
+    n_graph = sum(1 for r in r_graph if r.get("stage_graph"))
+    print(f"{precision} {opts}: {n_graph} of {len(r_graph)} iterations in stage graphs")
+    assert [r["c"] for r in r_graph] == [r["c"] for r in r_host]
+    assert [r["change"] for r in r_graph] == [r["change"] for r in r_host]
+    assert [r["lam"] for r in r_graph] == [r["lam"] for r in r_host]
+    assert [r["cg_iterations"] for r in r_graph] == [r["cg_iterations"] for r in r_host]
+    np.testing.assert_array_equal(x_graph, x_host)
+    assert c_graph == c_host
+    assert d_graph["projection_total_iterations"] == d_host["projection_total_iterations"]
+    if opts:
+        assert any(not r.get("stage_graph") for r in r_graph[1:])  # handed back to the host path
+    else:
+        assert n_graph >= len(r_graph) - 3  # all but the run's first body and rare hand-backs
