@@ -568,6 +568,11 @@ def run_batch(args):
     br.run(3 + max(1, args.warmup))
     conc_default = br.run(args.steps)
     br.close()
+    # every design advanced by one graph launch per call (no host thread per design)
+    br = BatchRunner(specs, precision=args.precision, workers=8, tune="bytes")
+    br.run_graph(max(1, args.warmup))
+    graph_tuned = br.run_graph(args.steps)
+    br.close()
     seq = BatchRunner(specs, precision=args.precision, workers=1, tune=None)
     seq.run(3 + max(1, args.warmup))
     one = seq.run(args.steps)
@@ -579,6 +584,9 @@ def run_batch(args):
                       "concurrent_8_threads_autotuned_bytes": tuned["bytes"],
                       "concurrent_8_threads_autotuned_time": tuned["time"],
                       "concurrent_8_threads_default_degrees": conc_default,
+                      "one_graph_launch_autotuned_bytes": graph_tuned,
+                      "speedup_graph_over_threads": graph_tuned["simp_iterations_per_s"]
+                      / tuned["bytes"]["simp_iterations_per_s"],
                       "one_after_another_default_degrees": one,
                       "speedup_concurrent": conc_default["simp_iterations_per_s"] / one["simp_iterations_per_s"],
                       "speedup_autotune_bytes": tuned["bytes"]["simp_iterations_per_s"]

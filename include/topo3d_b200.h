@@ -394,6 +394,24 @@ int tp3d_stage_run(tp3d_stage* g, void* stream, int* iterations, int* aborted);
 int tp3d_stage_count_launches(tp3d_stage* g, long long passes, long long cg_iterations);
 int tp3d_stage_destroy(tp3d_stage* g);
 
+/* Many designs in one graph launch: each design's loop body, as in the stage
+ * graph (its own solver, descriptor and buffers; counters and record per
+ * design), in a WHILE node of its own, the n loops parallel branches of one
+ * graph.  One launch advances every design by up to its counters' iteration
+ * limit (tolx < 0: exactly that many unless a solve is handed back); the
+ * designs share nothing but the GPU, whose scheduler overlaps their kernels as
+ * the branches allow.  The reference runs designs one after another
+ * (pytopo3d/runners/experiment.py); this has no counterpart there beyond the
+ * loop body. */
+typedef struct tp3d_batch tp3d_batch;
+int tp3d_batch_capture(tp3d_solver* const* solvers, const tp3d_stage_desc* descs, int n, void* stream,
+                       tp3d_batch** out);
+/* Launch on `stream` and wait; the caller reads each design's counters. */
+int tp3d_batch_run(tp3d_batch* b, void* stream);
+/* Add a run's kernel launches (per design: passes of the loop body, CG iterations) to tp3d_launch_count. */
+int tp3d_batch_count_launches(tp3d_batch* b, const long long* passes, const long long* cg_iterations);
+int tp3d_batch_destroy(tp3d_batch* b);
+
 /* Initial guess for the next solve of a load case from its last two solutions:
  * U <- 2 U - U_prev and U_prev <- (old) U; with have_prev == 0 only U_prev <- U.
  * Device arrays of n doubles.  The reference solves from scratch every

@@ -124,6 +124,10 @@ SIGNATURES = {
     "tp3d_stage_run": (i32, [vp, vp, C.POINTER(i32), C.POINTER(i32)]),
     "tp3d_stage_count_launches": (i32, [vp, i64, i64]),
     "tp3d_stage_destroy": (i32, [vp]),
+    "tp3d_batch_capture": (i32, [C.POINTER(vp), C.POINTER(StageDesc), i32, vp, C.POINTER(vp)]),
+    "tp3d_batch_run": (i32, [vp, vp]),
+    "tp3d_batch_count_launches": (i32, [vp, C.POINTER(i64), C.POINTER(i64)]),
+    "tp3d_batch_destroy": (i32, [vp]),
 }
 
 _lib = None

@@ -16,6 +16,7 @@ is ``SimpLoop.step`` (optimizer.py:578-696).
 
 from __future__ import annotations
 
+import ctypes as C
 import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
@@ -188,11 +189,95 @@ class BatchRunner:
         return {"seconds": dt, "designs": n, "iterations": iterations,
                 "simp_iterations_per_s": n * iterations / dt, "dof_cg_iterations_per_s": dof_cg / dt}
 
+    def run_graph(self, iterations: int) -> dict:
+        """Advance every design by ``iterations`` loop bodies with ONE graph
+        launch (``tp3d_batch_*``): each design's loop body in a WHILE node of its
+        own, all designs parallel branches of the graph, no host thread per
+        design.  Captured at the first call (every design must have run a loop
+        body on the host path, which the autotuning steps or ``run`` provide);
+        later calls relaunch it.  A design whose solve the host path would have
+        finished differently (the mixed form's FP64 fallback) is handed back:
+        its iteration is rerun on the host path and its remaining iterations
+        run there.  Returns the same figures as ``run``."""
+        from . import _lib
+        from .optimizer import stage_desc
+
+        n = len(self.specs)
+        if any(loop.S.n_iter == 0 for loop in self.loops):
+            self.run(1)
+        if getattr(self, "_graph", None) is None or iterations > self._graph_cap:
+            self._close_graph()
+            cap = max(int(iterations), 1)
+            self._graph_cap = cap
+            self._g_counters = torch.zeros((n, 8), dtype=torch.int32, device=device())
+            self._g_record = torch.zeros((n, cap, 8), dtype=torch.float64, device=device())
+            self._g_hold = []
+            descs = (_lib.StageDesc * n)()
+            handles = (C.c_void_p * n)()
+            for i, loop in enumerate(self.loops):
+                S = loop.S
+                loop.copy_mode = True
+                U_bak, rho_new = torch.empty_like(S.U), torch.empty_like(loop.x)
+                self._g_hold.append((U_bak, rho_new))
+                descs[i] = stage_desc(S, loop.x, loop.beta, loop.eta, loop.move, loop.target, -1.0,
+                                      self._g_counters[i], self._g_record[i], U_bak, rho_new)
+                handles[i] = S.solver._h
+            torch.cuda.synchronize()
+            h = C.c_void_p()
+            _lib.check(_lib.lib().tp3d_batch_capture(handles, descs, n, _lib.stream_ptr(), C.byref(h)),
+                       "batch_capture")
+            self._graph, self._g_descs = h, descs
+        torch.cuda.synchronize()
+        cg0 = list(self.cg_iterations)
+        t0 = time.perf_counter()
+        rows = [[0, 0, 0, int(iterations), loop.S.n_solved, 0, 0, 0] for loop in self.loops]
+        self._g_counters.copy_(torch.tensor(rows, dtype=torch.int32))
+        _lib.check(_lib.lib().tp3d_batch_run(self._graph, _lib.stream_ptr()), "batch_run")
+        ctr = self._g_counters.cpu().numpy()
+        rec = self._g_record.cpu().numpy()
+        passes = (C.c_longlong * n)()
+        cgs = (C.c_longlong * n)()
+        handed_back = 0
+        for i, loop in enumerate(self.loops):
+            it, ab = int(ctr[i, 0]), int(ctr[i, 1])
+            S = loop.S
+            S.n_solved += it
+            S.n_iter += it
+            cg = int(rec[i, :it, 5].sum())
+            passes[i], cgs[i] = it + ab, cg
+            c = float(rec[i, it - 1, 0]) if it else float("nan")
+            if ab:
+                handed_back += 1
+                with torch.cuda.stream(self.streams[i]):
+                    S.U.copy_(self._g_hold[i][0])
+                    st = loop.step(rerun=True)
+                    cg += loop.last["cg_iterations"]
+                    for _ in range(iterations - it - 1):
+                        st = loop.step()
+                        cg += loop.last["cg_iterations"]
+                    c = float(st[0])
+            self.cg_iterations[i] += cg
+            self.compliance[i] = c
+        _lib.lib().tp3d_batch_count_launches(self._graph, passes, cgs)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        dof_cg = sum(self.ndof[i] * (self.cg_iterations[i] - cg0[i]) for i in range(n))
+        return {"seconds": dt, "designs": n, "iterations": iterations, "handed_back": handed_back,
+                "simp_iterations_per_s": n * iterations / dt, "dof_cg_iterations_per_s": dof_cg / dt}
+
+    def _close_graph(self):
+        from . import _lib
+
+        if getattr(self, "_graph", None) is not None:
+            _lib.lib().tp3d_batch_destroy(self._graph)
+            self._graph = None
+
     def design(self, i: int) -> torch.Tensor:
         torch.cuda.synchronize()
         return self.loops[i].design()
 
     def close(self):
+        self._close_graph()
         for loop in self.loops:
             if loop is not None:
                 loop.close()

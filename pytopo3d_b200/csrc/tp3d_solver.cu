@@ -2636,21 +2636,11 @@ int stage_body(tp3d_solver* s, const tp3d_stage_desc* d, cudaStream_t cs, cudaSt
 
 }  // namespace
 
-extern "C" int tp3d_stage_capture(tp3d_solver* s, const tp3d_stage_desc* d, void* stream, tp3d_stage** out) {
-  if (!s || !d || !out || d->ncases < 1 || !d->F || !d->U || !d->U_prev || !d->U_bak || !d->x || !d->x_new ||
-      !d->rho_f || !d->rho_p || !d->dproj || !d->rho_new || !d->dc_dx || !d->dv_dx || !d->ce || !d->c || !d->Hs ||
-      !d->free_mask || !d->KE_host || !d->sens_scratch || !d->oc_scratch || !d->oc_stats || !d->record ||
-      !d->counters || (d->ncases > 1 && !d->dc_acc))
-    return TP3D_ERR_ARG;
-  if (!s->have_density || !s->fine_chosen || s->pending) {
-    tp3d_set_last_error("tp3d_stage_capture: run one loop body on the host path first");
-    return TP3D_ERR_ARG;
-  }
-  (void)stream;
-  *out = nullptr;
-  // what the capture needs but may not create while capturing: streams, the
-  // restart state, and the mixed form's FP64 fallback hierarchy (so that the
-  // captured set-up refreshes it exactly as the host path's does)
+namespace {
+// What a capture needs but may not create while capturing: streams, the
+// restart state, and the mixed form's FP64 fallback hierarchy (so that the
+// captured set-up refreshes it exactly as the host path's does).
+int stage_prepare(tp3d_solver* s) {
   if (!s->restart_state) s->restart_state = s->alloc<double>(4);
   if (!s->restart_state) return TP3D_ERR_CUDA;
   if (!s->st_loop) TP3D_CHECK(cudaStreamCreateWithFlags(&s->st_loop, cudaStreamNonBlocking));
@@ -2660,6 +2650,26 @@ extern "C" int tp3d_stage_capture(tp3d_solver* s, const tp3d_stage_desc* d, void
     if (int e = s->ensure_fp64_buffers()) return e;
     if (int e = s->leave()) return e;
   }
+  return TP3D_OK;
+}
+
+bool stage_desc_ok(const tp3d_stage_desc* d) {
+  return d && d->ncases >= 1 && d->F && d->U && d->U_prev && d->U_bak && d->x && d->x_new && d->rho_f && d->rho_p &&
+         d->dproj && d->rho_new && d->dc_dx && d->dv_dx && d->ce && d->c && d->Hs && d->free_mask && d->KE_host &&
+         d->sens_scratch && d->oc_scratch && d->oc_stats && d->record && d->counters &&
+         (d->ncases == 1 || d->dc_acc);
+}
+}  // namespace
+
+extern "C" int tp3d_stage_capture(tp3d_solver* s, const tp3d_stage_desc* d, void* stream, tp3d_stage** out) {
+  if (!s || !out || !stage_desc_ok(d)) return TP3D_ERR_ARG;
+  if (!s->have_density || !s->fine_chosen || s->pending) {
+    tp3d_set_last_error("tp3d_stage_capture: run one loop body on the host path first");
+    return TP3D_ERR_ARG;
+  }
+  (void)stream;
+  *out = nullptr;
+  if (int e = stage_prepare(s)) return e;
   cudaStream_t cs = nullptr, cs2 = nullptr;
   TP3D_CHECK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   TP3D_CHECK(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking));
@@ -2748,5 +2758,147 @@ extern "C" int tp3d_stage_destroy(tp3d_stage* g) {
   if (!g) return TP3D_OK;
   if (g->exec) cudaGraphExecDestroy(g->exec);
   delete g;
+  return TP3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Many designs in one graph launch: each design's loop body (as in the stage
+// graph above, its own solver and buffers) in a WHILE node of its own, all of
+// them parallel branches of one graph.  One launch advances every design by up
+// to its counters' iteration limit; the designs share nothing but the GPU, so
+// their kernels overlap as the graph's branches allow.  No host thread drives
+// a design while the graph runs.
+// ---------------------------------------------------------------------------
+struct tp3d_batch {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long long> body_kernels, loop_kernels;
+};
+
+extern "C" int tp3d_batch_capture(tp3d_solver* const* solvers, const tp3d_stage_desc* descs, int n, void* stream,
+                                  tp3d_batch** out) {
+  if (!solvers || !descs || !out || n < 1) return TP3D_ERR_ARG;
+  (void)stream;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    tp3d_solver* s = solvers[i];
+    if (!s || !stage_desc_ok(&descs[i])) return TP3D_ERR_ARG;
+    if (!s->have_density || !s->fine_chosen || s->pending) {
+      tp3d_set_last_error("tp3d_batch_capture: run one loop body of every design on the host path first");
+      return TP3D_ERR_ARG;
+    }
+    if (int e = stage_prepare(s)) return e;
+  }
+  std::vector<cudaStream_t> sts(3 * n + 1, nullptr);
+  std::vector<cudaEvent_t> evs(2 * n, nullptr);
+  for (auto& st : sts) TP3D_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  for (auto& ev : evs) TP3D_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  TP3D_CHECK(cudaDeviceSynchronize());
+  auto* b = new tp3d_batch();
+  b->body_kernels.assign(n, 0);
+  b->loop_kernels.assign(n, 0);
+  int rc = TP3D_OK;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    rc = TP3D_OK;
+    cudaStream_t root = sts[0];
+    cudaGraph_t G = nullptr;
+    if (cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    for (int i = 0; i < n && rc == TP3D_OK; ++i) {
+      tp3d_solver* s = solvers[i];
+      cudaStream_t br = sts[1 + 3 * i], body = sts[2 + 3 * i], ifs = sts[3 + 3 * i];
+      // fork a branch for design i from the graph's start (every branch waits on
+      // the same fork event, so no branch depends on another) and add its WHILE
+      // node there
+      if (i == 0 && cudaEventRecord(evs[0], root) != cudaSuccess) {
+        rc = TP3D_ERR_CUDA;
+        break;
+      }
+      if (cudaStreamWaitEvent(br, evs[0], 0) != cudaSuccess) {
+        rc = TP3D_ERR_CUDA;
+        break;
+      }
+      cudaStreamCaptureStatus cst;
+      cudaGraph_t capg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      cudaGraphConditionalHandle h = 0;
+      cudaGraphNodeParams cp = {};
+      cudaGraphNode_t wnode;
+      if (cudaStreamGetCaptureInfo(br, &cst, nullptr, &capg, &deps, &nd) != cudaSuccess ||
+          cudaGraphConditionalHandleCreate(&h, capg, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        rc = TP3D_ERR_CUDA;
+        break;
+      }
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      if (cudaGraphAddNode(&wnode, capg, deps, nd, &cp) != cudaSuccess ||
+          cudaStreamUpdateCaptureDependencies(br, &wnode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
+          cudaStreamBeginCaptureToGraph(body, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        rc = TP3D_ERR_CUDA;
+        break;
+      }
+      cudaStream_t saved_user = s->user;
+      s->user = body;
+      long long nk = 0;
+      t_capture_count = &nk;
+      rc = stage_body(s, &descs[i], body, ifs, h, &b->body_kernels[i]);
+      t_capture_count = nullptr;
+      b->body_kernels[i] += nk;
+      b->loop_kernels[i] = s->stage_loop_kernels;
+      s->user = saved_user;
+      cudaGraph_t ob = nullptr;
+      if (cudaStreamEndCapture(body, &ob) != cudaSuccess && rc == TP3D_OK) rc = TP3D_ERR_CUDA;
+      if (rc == TP3D_OK && cudaEventRecord(evs[2 * i + 1], br) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    }
+    // join every branch at the end
+    for (int i = 0; i < n && rc == TP3D_OK; ++i)
+      if (cudaStreamWaitEvent(root, evs[2 * i + 1], 0) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    if (cudaStreamEndCapture(root, &G) != cudaSuccess && rc == TP3D_OK) rc = TP3D_ERR_CUDA;
+    if (rc == TP3D_OK && cudaGraphInstantiate(&b->exec, G, 0) != cudaSuccess) rc = TP3D_ERR_CUDA;
+    if (G) cudaGraphDestroy(G);
+    cudaGetLastError();
+    if (rc == TP3D_OK) break;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->body_kernels.assign(n, 0);
+    bool any_pdl = false;
+    for (int i = 0; i < n; ++i) {
+      any_pdl = any_pdl || solvers[i]->pdl;
+      solvers[i]->pdl = false;  // retry in plain stream order
+    }
+    if (!any_pdl) break;
+  }
+  for (auto& st : sts) cudaStreamDestroy(st);
+  for (auto& ev : evs) cudaEventDestroy(ev);
+  if (rc) {
+    delete b;
+    if (!*tp3d_last_error()) tp3d_set_last_error("batch graph capture failed");
+    return rc;
+  }
+  *out = b;
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_batch_run(tp3d_batch* b, void* stream) {
+  if (!b || !b->exec) return TP3D_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  TP3D_CHECK(cudaGraphLaunch(b->exec, st));
+  TP3D_CHECK(cudaStreamSynchronize(st));
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_batch_count_launches(tp3d_batch* b, const long long* passes, const long long* cg_iterations) {
+  if (!b || !passes || !cg_iterations) return TP3D_ERR_ARG;
+  for (size_t i = 0; i < b->body_kernels.size(); ++i)
+    add_launches(passes[i] * b->body_kernels[i] + cg_iterations[i] * b->loop_kernels[i]);
+  return TP3D_OK;
+}
+
+extern "C" int tp3d_batch_destroy(tp3d_batch* b) {
+  if (!b) return TP3D_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  delete b;
   return TP3D_OK;
 }

@@ -198,6 +198,29 @@ class SimpState:
         return iters
 
 
+def stage_desc(S: "SimpState", x, beta, eta, move, target, tolx, counters, record, U_bak, rho_new,
+               max_bisection=80, bisection_tol=1e-8) -> "_lib.StageDesc":
+    """The tp3d_stage_desc of a loop state: its device buffers and the stage's
+    projection, OC and stopping parameters."""
+    d = _lib.StageDesc()
+    d.ncases = S.F.shape[0]
+    d.rmin, d.beta, d.eta, d.penal, d.move = float(S.H.rmin), float(beta), float(eta), S.penal, float(move)
+    d.target_free_volume, d.tolx = float(target), float(tolx)
+    d.max_bisection, d.bisection_tol = int(max_bisection), float(bisection_tol)
+    d.F, d.U, d.U_prev, d.U_bak = S.F.data_ptr(), S.U.data_ptr(), S.U_prev.data_ptr(), U_bak.data_ptr()
+    d.x, d.x_new = x.data_ptr(), S.x_new.data_ptr()
+    d.rho_f, d.rho_p, d.dproj, d.rho_new = S.rho_f.data_ptr(), S.rho_p.data_ptr(), S.dproj.data_ptr(), rho_new.data_ptr()
+    d.dc_dx, d.dc_acc, d.dv_dx, d.ce = S.dc_dx.data_ptr(), S.dc_acc.data_ptr(), S.dv_dx.data_ptr(), S.ce.data_ptr()
+    d.c = S.c_dev.data_ptr()
+    d.Hs = S.Hs.data_ptr()
+    d.solid, d.void_, d.free_mask = _lib.ptr(S.solid), _lib.ptr(S.void), S.free.data_ptr()
+    d.KE_host = S.KE.ctypes.data
+    d.sens_scratch, d.oc_scratch = S.sens_scratch.data_ptr(), S.ws.scratch.data_ptr()
+    d.oc_stats = S.ws.stats.data_ptr()
+    d.record, d.counters = record.data_ptr(), counters.data_ptr()
+    return d
+
+
 class StageGraph:
     """One projection stage of the loop body as a CUDA graph (tp3d_stage_*).
 
@@ -213,33 +236,16 @@ class StageGraph:
     def __init__(self, S: "SimpState", x, beta, eta, move, target, tolx, capacity,
                  max_bisection=80, bisection_tol=1e-8):
         self.S = S
-        n = x.numel()
         self.capacity = int(capacity)
         self.counters = torch.zeros(8, dtype=torch.int32, device=device())
         self.record = torch.zeros((self.capacity, 8), dtype=torch.float64, device=device())
         self.U_bak = torch.empty_like(S.U)
-        self.rho_new = torch.empty(n, dtype=torch.float64, device=device())
-        d = _lib.StageDesc()
-        d.ncases = S.F.shape[0]
-        d.rmin, d.beta, d.eta, d.penal, d.move = float(S.H.rmin), float(beta), float(eta), S.penal, float(move)
-        d.target_free_volume, d.tolx = float(target), float(tolx)
-        d.max_bisection, d.bisection_tol = int(max_bisection), float(bisection_tol)
-        d.F, d.U, d.U_prev, d.U_bak = S.F.data_ptr(), S.U.data_ptr(), S.U_prev.data_ptr(), self.U_bak.data_ptr()
-        d.x, d.x_new = x.data_ptr(), S.x_new.data_ptr()
-        d.rho_f, d.rho_p, d.dproj, d.rho_new = (S.rho_f.data_ptr(), S.rho_p.data_ptr(), S.dproj.data_ptr(),
-                                                self.rho_new.data_ptr())
-        d.dc_dx, d.dc_acc, d.dv_dx, d.ce = S.dc_dx.data_ptr(), S.dc_acc.data_ptr(), S.dv_dx.data_ptr(), S.ce.data_ptr()
-        d.c = S.c_dev.data_ptr()
-        d.Hs = S.Hs.data_ptr()
-        d.solid, d.void_, d.free_mask = _lib.ptr(S.solid), _lib.ptr(S.void), S.free.data_ptr()
-        d.KE_host = S.KE.ctypes.data
-        d.sens_scratch, d.oc_scratch = S.sens_scratch.data_ptr(), S.ws.scratch.data_ptr()
-        d.oc_stats = S.ws.stats.data_ptr()
-        d.record, d.counters = self.record.data_ptr(), self.counters.data_ptr()
-        self._desc = d
+        self.rho_new = torch.empty(x.numel(), dtype=torch.float64, device=device())
+        self._desc = stage_desc(S, x, beta, eta, move, target, tolx, self.counters, self.record, self.U_bak,
+                                self.rho_new, max_bisection, bisection_tol)
         self._x = x
         h = C.c_void_p()
-        _lib.check(_lib.lib().tp3d_stage_capture(S.solver._h, C.byref(d), _lib.stream_ptr(), C.byref(h)),
+        _lib.check(_lib.lib().tp3d_stage_capture(S.solver._h, C.byref(self._desc), _lib.stream_ptr(), C.byref(h)),
                    "stage_capture")
         self._h = h
 
@@ -307,6 +313,7 @@ class SimpLoop:
             self.x = to_flat(x0)
         self.beta = None
         self.last = {}
+        self.copy_mode = False  # a captured graph holds x's address: copy the new design, do not swap
         n = self.x.numel()
         self._pin_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
         self._pin_out = torch.empty(n + 1, dtype=torch.float64, pin_memory=True)
@@ -316,14 +323,18 @@ class SimpLoop:
         self.S.project(self.x, self.beta, self.eta)
         self.S.new_stage()
 
-    def step(self):
+    def step(self, rerun=False):
         """One loop body: solve, sensitivities, OC update, re-projection.
-        Returns the device stats tensor [c, lambda, volume, steps, change, ...]."""
+        Returns the device stats tensor [c, lambda, volume, steps, change, ...].
+        ``rerun``: the iteration a graph handed back (see SimpState.sensitivities)."""
         S = self.S
-        cg = S.sensitivities(S.rho_p, S.dproj)
+        cg = S.sensitivities(S.rho_p, S.dproj, rerun=rerun)
         stats = oc_update_flat(S.H, self.x, S.dc_dx, S.dv_dx, S.Hs, S.solid, S.void, self.move, self.target,
                                self.beta, self.eta, S.x_new, S.rho_new, S.ws)
-        self.x, S.x_new = S.x_new, self.x
+        if self.copy_mode:
+            self.x.copy_(S.x_new)
+        else:
+            self.x, S.x_new = S.x_new, self.x
         S.project(self.x, self.beta, self.eta)
         self.last = dict(cg_iterations=cg, relres=self.solver.last_relres)
         return torch.cat([S.c_dev[:1], stats])

@@ -63,3 +63,33 @@ def test_batch_designs_are_autotuned_one_by_one():
     stats = br.run(2)
     assert np.isfinite(br.compliance).all() and stats["dof_cg_iterations_per_s"] > 0
     br.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_graph_matches_host_runs(precision):
+    """All designs advanced by one graph launch (each design's loop body in a
+    WHILE node of its own, parallel branches) give exactly what each design's
+    host-driven loop gives, and a second launch continues them."""
+    from pytopo3d_b200.batch import BatchRunner, batched_cantilevers, design_problem
+    from pytopo3d_b200.optimizer import SimpLoop
+    from pytopo3d_b200.stiffness import lk_H8
+
+    specs = batched_cantilevers(5, seed=3)
+    opts = {"fine_operator": 3}
+    br = BatchRunner(specs, precision=precision, workers=1, solver_options=opts, tune=None)
+    br.run(1)
+    stats = br.run_graph(2)
+    assert stats["designs"] == 5 and stats["handed_back"] == 0
+    br.run_graph(2)
+    KE = lk_H8(elem_size=1.0)
+    for i, spec in enumerate(specs):
+        shape, solid, void, F, fixed = design_problem(spec)
+        loop = SimpLoop(spec.nelx, spec.nely, spec.nelz, spec.volfrac, spec.penal, spec.rmin, KE, F, fixed,
+                        solid, void, precision=precision, solver_options=opts)
+        loop.set_beta(1.0)
+        for _ in range(5):
+            st = loop.step()
+        assert float(st[0]) == br.compliance[i], i
+        np.testing.assert_array_equal(loop.design().cpu().numpy(), br.design(i).cpu().numpy())
+        loop.close()
+    br.close()
