@@ -69,6 +69,10 @@ def _validate_grid(nelx, nely, nelz, rmin):
         raise ValueError("nelx, nely, and nelz must all be positive")
     if not np.isfinite(rmin) or rmin <= 0.0:
         raise ValueError(f"rmin must be finite and positive, got {rmin}")
+    if rmin - 7.0 > 1e-9:
+        # the stencil reaches offsets d with rmin - d > 1e-9; its shared-memory
+        # tile holds offsets up to 6 per axis
+        raise ValueError(f"rmin too large for the stencil filter (max 7), got {rmin}")
 
 
 def filter_rowsum(H: ConeFilter) -> torch.Tensor:

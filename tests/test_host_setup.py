@@ -92,3 +92,11 @@ def test_top3d_validation_happens_before_any_device_work():
         kw.update(b)
         with pytest.raises(ValueError):
             top3d(**kw)
+
+
+def test_filter_radius_limit_is_reported_before_device_work():
+    from pytopo3d_b200.filter import _validate_grid
+
+    _validate_grid(4, 4, 4, 7.0)  # offsets up to 6: supported
+    with pytest.raises(ValueError, match="max 7"):
+        _validate_grid(4, 4, 4, 7.5)
