@@ -248,6 +248,12 @@ typedef struct tp3d_solver_opts {
                            FP64) */
   int spectra_streams;  /* 1 (default): each level's power iteration at set-up on its own stream, as
                            soon as the level is built; 0: all of them in order on the solver's stream */
+  int cluster_cycle;    /* mixed form, 1 (default): the two last smoothed levels and the coarsest solve
+                           run as one thread-block cluster of 8 (or 16) CTAs, each level's bf16
+                           stencil split over the CTAs' shared memory and the halos exchanged through
+                           distributed shared memory, when both levels hold bf16 stencils and the
+                           cluster fits; 0: the last smoothed level as one block (deep_cta) and the
+                           one before it one launch per smoothing step and transfer */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

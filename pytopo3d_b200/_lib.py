@@ -60,6 +60,7 @@ class SolverOpts(C.Structure):
         ("block_sweeps", i32),
         ("resid_restrict_dofs", i32),
         ("spectra_streams", i32),
+        ("cluster_cycle", i32),
     ]
 
 

@@ -54,12 +54,12 @@ __global__ void deep_pack_kernel(Grid g, const double* __restrict__ A, const uin
   }
 }
 
-// Part Q of K u at the three DOFs of node n from the node-major bf16 stencil
-// in shared memory: the entries of chunks 8Q .. 8Q+7.
+// Part Q of K u at the three DOFs of node n from its row of the node-major
+// bf16 stencil in shared memory: the entries of chunks 8Q .. 8Q+7.
 constexpr int kDeepPassNodes = 256;  // nodes per pass of the block: 8 groups of 32, four warps per group
 
 template <typename T, int Q>
-__device__ __forceinline__ void deep_node_part(const Grid& g, const __nv_bfloat16* SN, const T* u, int n, T y[3]) {
+__device__ __forceinline__ void deep_node_part(const Grid& g, const uint4* row, const T* u, int n, T y[3]) {
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const int NXY = NX * NY;
   const int iy = n % NY, r = n / NY;
@@ -67,7 +67,6 @@ __device__ __forceinline__ void deep_node_part(const Grid& g, const __nv_bfloat1
   const int oy0 = iy > 0 ? -1 : 0, oy2 = iy < NY - 1 ? 1 : 0;
   const int ox0 = ix > 0 ? -NY : 0, ox2 = ix < NX - 1 ? NY : 0;
   const int oz0 = iz > 0 ? -NXY : 0, oz2 = iz < NZ - 1 ? NXY : 0;
-  const uint4* row = reinterpret_cast<const uint4*>(SN + (size_t)n * kDeepRow);
   T acc[3][2] = {{T(0), T(0)}, {T(0), T(0)}, {T(0), T(0)}};
 #pragma unroll
   for (int q = 8 * Q; q < 8 * Q + 8 && q < kDeepRow / 8; ++q) {
@@ -241,11 +240,11 @@ __global__ void __launch_bounds__(kDeepThreads, 1) deep_cycle_kernel(const __gri
     const int n = base + nl;
     T y[3] = {T(0), T(0), T(0)};
     if (n < nn) {
-      const __nv_bfloat16* SN = reinterpret_cast<const __nv_bfloat16*>(S);
-      if (qp == 0) deep_node_part<T, 0>(p.g, SN, xv, n, y);
-      else if (qp == 1) deep_node_part<T, 1>(p.g, SN, xv, n, y);
-      else if (qp == 2) deep_node_part<T, 2>(p.g, SN, xv, n, y);
-      else deep_node_part<T, 3>(p.g, SN, xv, n, y);
+      const uint4* row = reinterpret_cast<const uint4*>(reinterpret_cast<const __nv_bfloat16*>(S) + (size_t)n * kDeepRow);
+      if (qp == 0) deep_node_part<T, 0>(p.g, row, xv, n, y);
+      else if (qp == 1) deep_node_part<T, 1>(p.g, row, xv, n, y);
+      else if (qp == 2) deep_node_part<T, 2>(p.g, row, xv, n, y);
+      else deep_node_part<T, 3>(p.g, row, xv, n, y);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) ypart[(qp * 3 + c) * kDeepPassNodes + nl] = y[c];

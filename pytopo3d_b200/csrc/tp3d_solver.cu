@@ -31,6 +31,7 @@
 #include "tp3d_fine_wht.cuh"
 #include "tp3d_coarse.cuh"
 #include "tp3d_deep.cuh"
+#include "tp3d_cluster.cuh"
 #include "tp3d_pcg.cuh"
 
 namespace tp3d {
@@ -328,6 +329,11 @@ struct tp3d_solver {
   size_t deep_smem = 0;
   bool deep_inv_smem = false;
   __nv_bfloat16* deep_SN = nullptr;  // its node-major bf16 stencil (bf16 levels)
+  // the two last smoothed levels (clu_L and deep_L = clu_L + 1) and the
+  // coarsest solve as one thread-block cluster of clu_C CTAs (mixed form; 0 none)
+  int clu_L = 0, clu_C = 0;
+  size_t clu_smem = 0;
+  __nv_bfloat16* clu_SN = nullptr;  // level clu_L's node-major bf16 stencil
   int cyc_blocks64 = 0, cyc_blocks32 = 0;
   unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
@@ -891,6 +897,62 @@ struct tp3d_solver {
     return lv.x[0];
   }
 
+  // Levels L, L + 1 and the coarsest solve as one thread-block cluster
+  // (cluster_cycle_kernel); the restriction that produced b took level L's
+  // first smoothing step.  Returns the buffer holding level L's iterate.
+  float* cluster_cycle(int L, const float* b, const int* done, int* rc) {
+    auto& la = L32[L];
+    auto& lb = L32[L + 1];
+    ClusterParams p;
+    p.gA = grids[L];
+    p.gB = grids[L + 1];
+    p.gC = grids[L + 2];
+    p.SA = clu_SN;
+    p.SB = deep_SN;
+    p.fixA = fix[L];
+    p.fixB = fix[L + 1];
+    p.fixC = fix[L + 2];
+    p.dinvA = la.dinv;
+    p.dinvB = lb.dinv;
+    p.coefA = coef[L];
+    p.coefB = coef[L + 1];
+    p.inv = cinv32;
+    p.cn = cn;
+    p.b = b;
+    p.x0 = la.x[0];
+    p.d0 = o.smoother != 1 ? la.d : nullptr;
+    p.xout = la.x[0];
+    p.preA = pre_sweeps(L);
+    p.postA = post_sweeps(L);
+    p.preB = pre_sweeps(L + 1);
+    p.postB = post_sweeps(L + 1);
+    p.cheb = o.smoother != 1;
+    p.omega = (float)o.omega;
+    p.done = done;
+    {
+      const double na = 3.0 * grids[L].nnode(), nb = 3.0 * grids[L + 1].nnode();
+      count_bytes(2.0 * kDeepRow / 3.0 * (na + nb) + 4.0 * cn * cn + 5.0 * sizeof(float) * na +
+                  (double)(grids[L].nnode() + grids[L + 1].nnode()));
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)clu_C);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.dynamicSmemBytes = clu_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)clu_C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = take_pdl(kPdlCoarse) ? 2 : 1;
+    if (cudaLaunchKernelEx(&cfg, cluster_cycle_kernel, p) != cudaSuccess) *rc = TP3D_ERR_CUDA;
+    count_launch();
+    return la.x[0];
+  }
+
   // V-cycle on level L with right-hand side b; returns the buffer holding x.
   template <typename T>
   // zero_done: the first smoothing step from zero already ran (fused into the
@@ -920,8 +982,10 @@ struct tp3d_solver {
       return lv.x[0];
     }
     if (L == cyc_L0 && cyc_L0 > 0) return coarse_cycle<T>(L, b, rc);
-    if constexpr (sizeof(T) == 4)
+    if constexpr (sizeof(T) == 4) {
+      if (L == clu_L && clu_L > 0 && zero_done) return cluster_cycle(L, b, done, rc);
       if (L == deep_L && deep_L > 0 && zero_done) return deep_cycle(L, b, done, rc);
+    }
     const bool cheb = o.smoother != 1;
     int cur = 0;
     if (!zero_done) {
@@ -1762,6 +1826,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->block_sweeps = 0;
   o->resid_restrict_dofs = 0;
   o->spectra_streams = 1;
+  o->cluster_cycle = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1995,6 +2060,45 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
     }
     cudaGetLastError();
   }
+  // the two last smoothed levels and the coarsest solve as one cluster, when
+  // both levels hold bf16 stencils and a cluster of 8 (or 16) CTAs holds them
+  if (mixed && o.cluster_cycle && s->deep_L >= 2 && s->deep_SN && s->S16[s->deep_L - 1]) {
+    const int L = s->deep_L - 1;
+    const int nA = (int)s->grids[L].nnode(), nB = (int)s->grids[L + 1].nnode(), nC = (int)s->grids[L + 2].nnode();
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    for (int C : {8, 16}) {
+      const size_t smem = cl_layout(nA, nB, nC, C).total;
+      if (smem > (size_t)optin || nC < C) continue;
+      if (ensure_dynamic_smem(cluster_cycle_kernel, smem) != TP3D_OK) break;
+      if (C > 8 && cudaFuncSetAttribute(cluster_cycle_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                       cudaSuccess)
+        break;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)C);
+      cfg.blockDim = dim3(kClThreads);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)C;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, cluster_cycle_kernel, &cfg) != cudaSuccess || nclusters < 1)
+        continue;
+      s->clu_SN = s->alloc<__nv_bfloat16>((size_t)nA * kDeepRow);
+      if (s->clu_SN) {
+        s->clu_L = L;
+        s->clu_C = C;
+        s->clu_smem = smem;
+      }
+      break;
+    }
+    cudaGetLastError();
+  }
   if (cudaStreamSynchronize(s->st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
     return fail(TP3D_ERR_CUDA, "setup failed");
   *out = s;
@@ -2209,6 +2313,10 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     }
     if (L == s->deep_L && s->deep_SN) {
       deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->deep_SN);
+      count_launch();
+    }
+    if (L == s->clu_L && s->clu_SN) {
+      deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->clu_SN);
       count_launch();
     }
     TP3D_CHECK_LAUNCH();
@@ -2526,7 +2634,8 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)s->tuned, (double)s->o.pre_sweeps, (double)s->pre_sweeps(1),
                            (double)s->pre_sweeps(2),
                            (double)(s->mixed ? (s->use_wht32 ? s->wt32.ZC : 0) : (s->use_wht64 ? s->wt64.ZC : 0)),
-                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.nthr : 0) : (s->use_wht64 ? s->wt64.nthr : 0))};
+                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.nthr : 0) : (s->use_wht64 ? s->wt64.nthr : 0)),
+                           (double)s->clu_L, (double)s->clu_C};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

@@ -153,7 +153,7 @@ class HexSolver:
                 "fp64_fallback", "fine_form_fp64", "fine_form_fp32", "fused_cycle_level", "device_loop",
                 "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level", "bytes_per_cg_iteration",
                 "kernels_per_cg_iteration", "autotuned", "degree_fine", "degree_level1", "degree_level2",
-                "fine_slab_depth", "fine_threads"]
+                "fine_slab_depth", "fine_threads", "cluster_level", "cluster_ctas"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
 
     def autotune(self, F: torch.Tensor, U0: Optional[torch.Tensor] = None, criterion: Optional[str] = None) -> dict:

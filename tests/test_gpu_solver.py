@@ -276,6 +276,39 @@ def test_deep_block_cycle_matches_per_phase_launches(P, dims, fits, smoother):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
 
 
+# The two last smoothed levels and the coarsest solve as one thread-block
+# cluster (cluster_cycle) against the same levels as per-phase launches plus
+# the one-block deep cycle: the same operations, the level before the block
+# summed in another order, so the same iterations (within one or 2%) and the
+# same solution to rounding.  (16, 8, 8) has too few levels for a cluster.
+@pytest.mark.parametrize("dims,used", [((64, 32, 32), True), ((32, 16, 16), True), ((128, 64, 64), True),
+                                       ((62, 30, 34), True), ((16, 8, 8), False)])
+def test_cluster_cycle_matches_block_cycle(P, dims, used):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=9)
+    rho[rho < 0.25] = 0.0
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    its, Us = [], []
+    for clu in (0, 1):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", cluster_cycle=clu, fine_operator=3)
+        s.set_density(to_flat(rho), 3.0)
+        st = s.stats()
+        if clu and used:
+            assert st["cluster_level"] == st["levels"] - 3 and st["cluster_ctas"] in (8, 16), st
+        else:
+            assert st["cluster_level"] == 0, st
+        U = s.solve(F)
+        its.append(s.last_iterations)
+        Us.append(U.cpu().numpy())
+        s.close()
+    assert abs(its[0] - its[1]) <= max(1, 0.02 * its[0]), its
+    np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
+
+
 # Residual and restriction in one launch on the small levels are the same
 # operations as the two launches, summed in another order: same iterations
 # (within one or 2%), same solution to rounding.
