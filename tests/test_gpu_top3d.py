@@ -202,3 +202,78 @@ def test_stage_graph_matches_host_path(P, precision, opts):
         assert any(not r.get("stage_graph") for r in r_graph[1:])  # handed back to the host path
     else:
         assert n_graph >= len(r_graph) - 3  # all but the run's first body and rare hand-backs
+
+
+@pytest.fixture(scope="module")
+def cantilever_run(P):
+    """The 32x16x16 cantilever in full (beta 1, 2, 4, 8; maxloop 200 per stage;
+    tolx 0.01; volfrac 0.3; penal 3; rmin 3; the reference's default load and
+    supports) with the FP64 solver at a relative residual of 1e-12."""
+    import os
+
+    from pytopo3d_b200._tensors import from_flat
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "golden_cantilever_32x16x16.npz"))
+    rec, diag = [], {}
+    xphys, hist, comp, failure = P.top3d(nelx=32, nely=16, nelz=16, volfrac=0.3, penal=3.0, rmin=3.0,
+                                         disp_thres=0.5, elem_size=1.0, tolx=0.01, maxloop=200,
+                                         beta_schedule=(1.0, 2.0, 4.0, 8.0), save_history=True,
+                                         history_frequency=1, diagnostics_out=diag, record=rec,
+                                         solver_options={"rtol": 1e-12, "max_iterations": 20000})
+    shape = (16, 32, 16)
+    x = [from_flat(e["x"], shape).cpu().numpy() for e in rec]
+    return g, dict(xphys=xphys, hist=hist, comp=comp, failure=failure, diag=diag, rec=rec, x=x)
+
+
+def test_cantilever_full_run_matches_reference(cantilever_run):
+    """The whole 800-iteration run against the reference's own run of the same
+    problem (``golden_cantilever_32x16x16.npz``, recorded by
+    tests/golden/make_golden.py from pytopo3d/core/optimizer.py:537-836 with
+    its direct solve): the same stage lengths and stopping, the first ten
+    designs, the design at the end of every stage, the compliance of every
+    iteration, the final physical density and compliance, and the stage
+    diagnostics.  The B200 solves iteratively (FP64 CG to relres 1e-12) and
+    sums the filter and the volume in another order, so the runs start
+    1e-12 apart and the OC bisection carries the difference along the
+    trajectory.  Measured on a B200: first ten designs 1.1e-11, stage-end
+    designs 1.6e-9 / 9.1e-9 / 6.4e-9 / 2.2e-8, compliance of every iteration
+    7.8e-10 relative (9.5e-12 over the first ten), change 4.2e-8, final
+    physical density 2.9e-9, final compliance 1.3e-10; the bounds are about
+    ten times those (the test prints them)."""
+    g, r = cantilever_run
+    diag, rec, hist = r["diag"], r["rec"], r["hist"]
+    assert r["failure"] is None
+    st = diag["projection_stage_summaries"]
+    np.testing.assert_array_equal([s["iterations"] for s in st], g["cl_stage_iterations"])
+    assert diag["projection_total_iterations"] == int(g["cl_total_iterations"]) == len(rec)
+    err_first = np.abs(np.stack(r["x"][:10]) - g["cl_first_x"]).max()
+    ends = np.cumsum(g["cl_stage_iterations"]) - 1
+    err_ends = [float(np.abs(r["x"][i] - g["cl_stage_end_x"][k]).max()) for k, i in enumerate(ends)]
+    c = np.array(hist["compliance_history"])
+    c_ref = g["cl_hist_c"]
+    assert c.shape == c_ref.shape
+    err_c = np.abs(c / c_ref - 1.0)
+    err_change = np.abs(np.array([e["change"] for e in rec]) - g["cl_change"])
+    err_xphys = np.abs(r["xphys"] - g["cl_xphys"]).max()
+    err_comp = abs(r["comp"] / float(g["cl_compliance"]) - 1.0)
+    print(f"first 10 designs {err_first:.2e}; stage-end designs {['%.2e' % e for e in err_ends]}; "
+          f"compliance per iteration: first 10 {err_c[:10].max():.2e}, stage 1 {err_c[:200].max():.2e}, "
+          f"all {err_c.max():.2e}; change {err_change.max():.2e}; xphys {err_xphys:.2e}; "
+          f"final compliance {err_comp:.2e}")
+    assert err_first <= 1e-10
+    assert err_c[:10].max() <= 1e-10
+    assert err_c.max() <= 1e-8
+    assert max(err_ends) <= 3e-7
+    assert err_change.max() <= 5e-7
+    assert err_xphys <= 3e-8
+    assert err_comp <= 2e-9
+    np.testing.assert_allclose([s["physical_density_fraction"] for s in st], g["cl_stage_vol"], atol=1e-10)
+    # a count of elements: at most one element's density may sit on 0.05 or 0.95 differently
+    np.testing.assert_allclose([s["gray_fraction_005_095"] for s in st], g["cl_stage_gray"], atol=1.0 / 8192)
+    np.testing.assert_allclose([s["minimum_achievable_physical_fraction"] for s in st], g["cl_stage_vmin"],
+                               atol=1e-8)
+    np.testing.assert_allclose([s["maximum_achievable_physical_fraction"] for s in st], g["cl_stage_vmax"],
+                               atol=1e-12)
+    np.testing.assert_allclose([s["final_change"] for s in st], g["cl_stage_final_change"], atol=5e-7)
+    assert diag["binary_compliance"] == pytest.approx(float(g["cl_binary_compliance"]), rel=1e-6)

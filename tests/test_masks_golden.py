@@ -112,3 +112,21 @@ def test_mask_validation_messages():
         resolve_masks(3, 2, 2, support_mask=np.zeros((3, 2, 2), bool))
     with pytest.raises(ValueError, match="at least one free design element"):
         resolve_masks(3, 2, 2, protected_zone_mask=np.ones(shape, bool))
+
+
+def test_cantilever_masks_loads_and_supports_bit_exact():
+    """The 32x16x16 cantilever run in full (``golden_cantilever_32x16x16.npz``):
+    default masks, load and supports as the reference built them."""
+    g = np.load(os.path.join(ROOT, "golden", "golden_cantilever_32x16x16.npz"))
+    nx, ny, nz = 32, 16, 16
+    solid, void, free = resolve_masks(nx, ny, nz)
+    np.testing.assert_array_equal(solid, g["cl_solid"])
+    np.testing.assert_array_equal(void, g["cl_void"])
+    np.testing.assert_array_equal(free, g["cl_free"])
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    F = P.build_force_vector(nx, ny, nz, ndof)
+    idx = np.flatnonzero(F)
+    np.testing.assert_array_equal(idx, g["cl_F_idx"])
+    np.testing.assert_array_equal(F[idx], g["cl_F_val"])
+    free_dofs, _ = P.build_supports(nx, ny, nz, ndof)
+    np.testing.assert_array_equal(free_dofs, g["cl_freedofs"])
