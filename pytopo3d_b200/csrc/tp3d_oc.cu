@@ -21,6 +21,7 @@ namespace tp3d {
 namespace {
 
 constexpr int kOcMaxBlocks = 4096;
+constexpr int kOcBatch = 8;  // staged candidates per thread whose loads are in flight together
 
 struct OcArgs {
   Grid g;
@@ -86,17 +87,33 @@ __device__ bool oc_volume(const OcArgs& a, double lam, double* part, double* s, 
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const FilterTile tile = filter_tile_at(a.g, t);
     __syncthreads();
-#pragma unroll 4
-    for (int i = threadIdx.x; i < NS; i += kFilterThreads) {
-      const int ly = i % SY, r = i / SY;
-      const int lx = r % SX, lz = r / SX;
-      const int gx = tile.x0 + lx - Z, gy = tile.y0 + ly - Z, gz = tile.z0 + lz - Z;
-      double v = 0.0;
-      if (gx >= 0 && gx < a.g.nx && gy >= 0 && gy < a.g.ny && gz >= 0 && gz < a.g.nz) {
-        const long long e = a.g.eidx(gx, gy, gz);
-        v = candidate_q(__ldg(&a.x[e]), __ldcg(&a.ratio[e]), isl, a.move);
+    // kOcBatch elements per thread at a time: all their loads are issued
+    // before the first candidate is formed, so they are in flight together
+    for (int i0 = threadIdx.x; i0 < NS; i0 += kOcBatch * kFilterThreads) {
+      double xv[kOcBatch], qv[kOcBatch];
+      unsigned in = 0;
+#pragma unroll
+      for (int b = 0; b < kOcBatch; ++b) {
+        const int i = i0 + b * kFilterThreads;
+        xv[b] = 0.0;
+        qv[b] = 0.0;
+        if (i < NS) {
+          const int ly = i % SY, r = i / SY;
+          const int lx = r % SX, lz = r / SX;
+          const int gx = tile.x0 + lx - Z, gy = tile.y0 + ly - Z, gz = tile.z0 + lz - Z;
+          if (gx >= 0 && gx < a.g.nx && gy >= 0 && gy < a.g.ny && gz >= 0 && gz < a.g.nz) {
+            const long long e = a.g.eidx(gx, gy, gz);
+            xv[b] = __ldg(&a.x[e]);
+            qv[b] = __ldcg(&a.ratio[e]);
+            in |= 1u << b;
+          }
+        }
       }
-      s[i] = v;
+#pragma unroll
+      for (int b = 0; b < kOcBatch; ++b) {
+        const int i = i0 + b * kFilterThreads;
+        if (i < NS) s[i] = ((in >> b) & 1u) ? candidate_q(xv[b], qv[b], isl, a.move) : 0.0;
+      }
     }
     __syncthreads();
     filter_apply<Z>(a.g, a.fc, tile, s, [&](long long e, int, int, int, double v) {
