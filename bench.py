@@ -436,11 +436,13 @@ def main():
     achieved = alg_bytes / (main_r["apply_ms"] * 1e-3) / 1e9
     nnode = (NELX + 1) * (NELY + 1) * (NELZ + 1)
     form = main_r["stats"].get("fine_form_fp32" if fp32 else "fine_form_fp64", 0)
-    kname = "wht_apply" if form and form >= 1 else "fine_apply"
+    # fine_form is 1 + the Walsh-Hadamard shape (0 the dense form); FP32 shapes
+    # 6 and 7 run Apply in the one-barrier kernel
+    kname = ("wht1_apply" if fp32 and form >= 7 else "wht_apply") if form and form >= 1 else "fine_apply"
     # floating-point operations the kernel executes per node (FMA = 2): the
     # Walsh-Hadamard block form does 99 FMAs and 81 adds per node and plane; the
     # dense-KE form the dense 576 FMAs per element
-    flops_node = 279.0 if kname == "wht_apply" else 1152.0
+    flops_node = 1152.0 if kname == "fine_apply" else 279.0
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):

@@ -203,9 +203,10 @@ typedef struct tp3d_solver_opts {
                            set_density; 1 dense KE; 2 Walsh-Hadamard (fastest shape); 3 + v the
                            Walsh-Hadamard form with shape v only (FP64: v = 0..2; FP32: v = 0..2 the
                            packed two-plane kernel with paired FP32 instructions, 3..5 the scalar
-                           kernel; the timed choices 0 and 2 consider only the scalar FP32 shapes,
-                           which measured faster).  The block form needs an axis-aligned orthotropic
-                           KE and falls back to the dense form otherwise. */
+                           two-barrier kernel, 6..7 the one-barrier kernel for the apply, residual,
+                           CG-product and power-iteration modes; the timed choices 0 and 2 skip the
+                           packed shapes, which measured slower).  The block form needs an
+                           axis-aligned orthotropic KE and falls back to the dense form otherwise. */
   int fused_cycle_dofs; /* the V-cycle from the first level (>= 1) with at most this many DOFs down
                            to the coarsest runs as one cooperative launch with grid barriers;
                            0 (default) keeps one launch per smoothing step and transfer, which
@@ -254,6 +255,9 @@ typedef struct tp3d_solver_opts {
                            distributed shared memory, when both levels hold bf16 stencils and the
                            cluster fits; 0: the last smoothed level as one block (deep_cta) and the
                            one before it one launch per smoothing step and transfer */
+  int fine_slab_depth;  /* Walsh-Hadamard fine operator: node planes per block along z; 0 (default)
+                           the fastest of the tile model's depth, half of it and twice it, timed with
+                           the launch shapes; > 0 that depth only (profiling, reproducible tiles) */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

@@ -61,6 +61,7 @@ class SolverOpts(C.Structure):
         ("resid_restrict_dofs", i32),
         ("spectra_streams", i32),
         ("cluster_cycle", i32),
+        ("fine_slab_depth", i32),
     ]
 
 

@@ -5,38 +5,56 @@
 #include <cmath>
 
 #include "tp3d_fine_wht.cuh"
+#include "tp3d_fine_wht1.cuh"
 #include "tp3d_fine_wht2.cuh"
 
 namespace tp3d {
 
 namespace {
 
-// (threads, min blocks per SM) of each variant, per precision
+// (threads, min blocks per SM, kernel) of each variant, per precision.
+// Kernels: 0 the scalar two-barrier kernel (tp3d_fine_wht.cuh), 1 the packed
+// FP32 two-plane kernel (tp3d_fine_wht2.cuh, twice the scalar kernel's
+// per-thread state, so fewer threads per block), 2 the one-barrier kernel
+// (tp3d_fine_wht1.cuh) for the epilogue modes of wht1_mode() and the
+// two-barrier kernel for the others (same tile, same results).  The timed
+// choice considers kernels 0 and 2.
+enum : int { kWhtScalar = 0, kWhtPacked = 1, kWhtOneBarrier = 2 };
 template <typename T>
 struct WhtShapes;
-// FP32 offers the packed two-plane kernel (tp3d_fine_wht2.cuh, twice the scalar
-// kernel's per-thread state, so fewer threads per block) and the scalar one
-// variants 0-2 the packed kernel, 3-5 the scalar one (both are timed)
 template <>
 struct WhtShapes<float> {
-  static constexpr int count = 6;
-  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 512, 768, 256};
-  static constexpr int minb[kWhtVariants] = {1, 1, 3, 2, 1, 4};
-  static constexpr bool packed[kWhtVariants] = {true, true, true, false, false, false};
+  static constexpr int count = 8;
+  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 512, 768, 256, 256, 512};
+  static constexpr int minb[kWhtVariants] = {1, 1, 3, 2, 1, 4, 4, 2};
+  static constexpr int kind[kWhtVariants] = {kWhtPacked, kWhtPacked, kWhtPacked,     kWhtScalar,
+                                             kWhtScalar, kWhtScalar, kWhtOneBarrier, kWhtOneBarrier};
 };
+template <>
+struct WhtShapes<double> {
+  static constexpr int count = 3;
+  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 256, 256, 256, 256, 256};
+  static constexpr int minb[kWhtVariants] = {2, 1, 4, 2, 2, 2, 2, 2};
+  static constexpr int kind[kWhtVariants] = {kWhtScalar, kWhtScalar, kWhtScalar, kWhtScalar,
+                                             kWhtScalar, kWhtScalar, kWhtScalar, kWhtScalar};
+};
+
+// Epilogue modes that the one-barrier shapes run in the one-barrier kernel:
+// the plain apply, the residual, the CG product and the power-iteration step.
+// The Chebyshev and Jacobi steps (up to nine epilogue inputs per node) spill
+// in it under 64 registers per thread and measured faster in the two-barrier
+// kernel (128x64x64 SIMP step: 8.98 ms with this split, 9.10 ms with every
+// mode in the one-barrier kernel, 9.02 ms with none).
+constexpr bool wht1_mode(int mode) {
+  return mode == kModeApply || mode == kModeResid || mode == kModeCgQ || mode == kModeDinvApply;
+}
 
 // dynamic shared memory of a launch of variant v
 template <typename T>
 constexpr size_t wht_kernel_smem(int v) {
-  return WhtShapes<T>::packed[v] ? wht2_smem_bytes(WhtShapes<T>::nthr[v]) : wht_smem_bytes<T>(WhtShapes<T>::nthr[v]);
+  const int k = WhtShapes<T>::kind[v], n = WhtShapes<T>::nthr[v];
+  return k == kWhtPacked ? wht2_smem_bytes(n) : (k == kWhtOneBarrier ? wht1_smem_bytes<T>(n) : wht_smem_bytes<T>(n));
 }
-template <>
-struct WhtShapes<double> {
-  static constexpr int count = 3;
-  static constexpr int nthr[kWhtVariants] = {256, 384, 128, 256, 384, 128};
-  static constexpr int minb[kWhtVariants] = {2, 1, 4, 2, 1, 4};
-  static constexpr bool packed[kWhtVariants] = {false, false, false, false, false, false};
-};
 
 template <typename T, class ESrc, int V>
 struct WhtVariant {
@@ -44,7 +62,10 @@ struct WhtVariant {
   static constexpr int MINB = WhtShapes<T>::minb[V];
   template <int MODE>
   static void* fn() {
-    if constexpr (WhtShapes<T>::packed[V]) return (void*)wht2_apply_kernel<ESrc, MODE, NTHR, MINB>;
+    constexpr int K = WhtShapes<T>::kind[V];
+    if constexpr (K == kWhtPacked) return (void*)wht2_apply_kernel<ESrc, MODE, NTHR, MINB>;
+    else if constexpr (K == kWhtOneBarrier && wht1_mode(MODE))
+      return (void*)wht1_apply_kernel<T, ESrc, MODE, NTHR, MINB>;
     else return (void*)wht_apply_kernel<T, ESrc, MODE, NTHR, MINB>;
   }
   static void* by_mode(int mode) {
@@ -68,6 +89,8 @@ void* wht_fn(int mode, int v) {
       case 3: return WhtVariant<T, ESrc, 3>::by_mode(mode);
       case 4: return WhtVariant<T, ESrc, 4>::by_mode(mode);
       case 5: return WhtVariant<T, ESrc, 5>::by_mode(mode);
+      case 6: return WhtVariant<T, ESrc, 6>::by_mode(mode);
+      case 7: return WhtVariant<T, ESrc, 7>::by_mode(mode);
       default: break;
     }
   }
@@ -98,6 +121,11 @@ int wht_variant_threads(int v) {
 template <typename T, class ESrc>
 int wht_variant_count() {
   return WhtShapes<T>::count;
+}
+
+template <typename T, class ESrc>
+bool wht_variant_timed(int v) {
+  return v >= 0 && v < WhtShapes<T>::count && WhtShapes<T>::kind[v] != kWhtPacked;
 }
 
 template <typename T, class ESrc>
@@ -205,6 +233,7 @@ WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
 #define TP3D_WHT_INSTANTIATE(T, ESrc)                                                     \
   template int wht_variant_threads<T, ESrc>(int);                                        \
   template int wht_variant_count<T, ESrc>();                                             \
+  template bool wht_variant_timed<T, ESrc>(int);                                         \
   template int wht_occupancy<T, ESrc>(int);                                              \
   template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t, bool); \
   template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);

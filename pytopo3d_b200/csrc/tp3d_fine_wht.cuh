@@ -247,11 +247,12 @@ __global__ void __launch_bounds__(NTHR, MINB) wht_apply_kernel(const __grid_cons
 namespace tp3d {
 
 // Block shapes offered for the Walsh-Hadamard operator (threads, minimum
-// resident blocks per SM; for FP32 the packed two-plane kernel and the scalar
-// one).  Explicit instantiations live in tp3d_fine_wht.cu; the solver times
+// resident blocks per SM, and the kernel: the scalar two-barrier kernel, the
+// one-barrier kernel of tp3d_fine_wht1.cuh, for FP32 also the packed two-plane
+// kernel).  Explicit instantiations live in tp3d_fine_wht.cu; the solver times
 // them on its own grid and keeps the fastest.  kWhtVariants is the most any
 // precision offers (wht_variant_count).
-constexpr int kWhtVariants = 6;
+constexpr int kWhtVariants = 8;
 
 // Host view of one launch configuration.
 struct WhtTile {
@@ -263,6 +264,9 @@ template <typename T, class ESrc>
 int wht_variant_threads(int v);
 template <typename T, class ESrc>
 int wht_variant_count();
+// false for shapes that the timed choice skips (taken only when asked for by name)
+template <typename T, class ESrc>
+bool wht_variant_timed(int v);
 template <typename T, class ESrc>
 int wht_occupancy(int v);
 template <typename T, class ESrc>

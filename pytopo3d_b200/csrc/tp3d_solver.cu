@@ -73,9 +73,10 @@ constexpr int kPdlCoarse = 1, kPdlFine = 2;  // tp3d_solver_opts::pdl bits
 // Process-wide caches of tuning choices (fine operator form and tile; the
 // smoothing degrees of the autotuner), keyed by the grid and precision.
 struct FineChoiceKey {
-  int nx, ny, nz, tsize, bf16, form_opt;
+  int nx, ny, nz, tsize, bf16, form_opt, slab_opt;
   bool operator<(const FineChoiceKey& o) const {
-    return std::tie(nx, ny, nz, tsize, bf16, form_opt) < std::tie(o.nx, o.ny, o.nz, o.tsize, o.bf16, o.form_opt);
+    return std::tie(nx, ny, nz, tsize, bf16, form_opt, slab_opt) <
+           std::tie(o.nx, o.ny, o.nz, o.tsize, o.bf16, o.form_opt, o.slab_opt);
   }
 };
 struct FineChoice {
@@ -614,7 +615,7 @@ struct tp3d_solver {
     WhtTile& wt = sizeof(T) == 8 ? wt64 : wt32;
     use = false;
     if (!wht_ok) return TP3D_OK;
-    const FineChoiceKey key{g.nx, g.ny, g.nz, (int)sizeof(T), rho16 ? 1 : 0, o.fine_operator};
+    const FineChoiceKey key{g.nx, g.ny, g.nz, (int)sizeof(T), rho16 ? 1 : 0, o.fine_operator, o.fine_slab_depth};
     {
       std::lock_guard<std::mutex> lk(fine_choice_mu());
       auto it = fine_choice_cache().find(key);
@@ -636,13 +637,18 @@ struct tp3d_solver {
     else nvar = wht_variant_count<float, EFromF32>();
     for (int v = 0; v < nvar && rc == TP3D_OK; ++v) {
       if (o.fine_operator > 2 && v != o.fine_operator - 3) continue;
-      // the packed FP32 shapes (0-2) are taken only when asked for by name: on
-      // B200 they measured slower than the scalar ones (150 registers per thread,
-      // a quarter of the resident warps), so the timed choice skips them
-      if (o.fine_operator <= 2 && nvar > 3 && v < 3) continue;
+      // the packed FP32 shapes are taken only when asked for by name: on B200
+      // they measured slower than the scalar ones (150 registers per thread, a
+      // quarter of the resident warps), so the timed choice skips them
+      bool timed;
+      if constexpr (sizeof(T) == 8) timed = wht_variant_timed<double, EFromF64>(v);
+      else timed = wht_variant_timed<float, EFromF32>(v);
+      if (o.fine_operator <= 2 && !timed) continue;
       const WhtTile base = wht_tile_for<T>(v);
       int zcs[3] = {base.ZC, std::max(1, base.ZC / 2), std::min(NZ, 2 * base.ZC)};
-      for (int k = 0; k < 3 && rc == TP3D_OK; ++k) {
+      const int nzc = o.fine_slab_depth > 0 ? 1 : 3;
+      if (o.fine_slab_depth > 0) zcs[0] = std::min(NZ, o.fine_slab_depth);
+      for (int k = 0; k < nzc && rc == TP3D_OK; ++k) {
         if (k > 0 && (zcs[k] == base.ZC || (k == 2 && zcs[2] == zcs[1]))) continue;
         WhtTile w = base;
         w.ZC = zcs[k];
@@ -1827,6 +1833,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->resid_restrict_dofs = 0;
   o->spectra_streams = 1;
   o->cluster_cycle = 1;
+  o->fine_slab_depth = 0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1876,6 +1883,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   s->ke_cls = ke_classes(KE_host, s->kcls64);
   if (o.fine_operator < 0 || o.fine_operator > 2 + kWhtVariants)
     return fail(TP3D_ERR_ARG, "invalid fine_operator option");
+  if (o.fine_slab_depth < 0) return fail(TP3D_ERR_ARG, "invalid fine_slab_depth option");
   {
     double m[8][3][3];
     s->wht_ok = o.fine_operator != 1 && wht_blocks_from_ke(KE_host, m);

@@ -81,10 +81,11 @@ def test_apply_matches_assembled_matrix(P, dims, form):
 
 
 # FP32 Walsh-Hadamard shapes: 0-2 the packed two-plane kernel (paired FP32
-# instructions), 3-5 the scalar kernel.  Odd plane counts per block and grids
-# spanning several tiles and z chunks; the apply against the assembled FP64
-# operator, and a mixed solve (every epilogue mode of the kernel) against FP64.
-@pytest.mark.parametrize("shape", range(6))
+# instructions), 3-5 the scalar two-barrier kernel, 6-7 the one-barrier kernel.
+# Odd plane counts per block and grids spanning several tiles and z chunks; the
+# apply against the assembled FP64 operator, and a mixed solve (every epilogue
+# mode of the kernel) against FP64.
+@pytest.mark.parametrize("shape", range(8))
 @pytest.mark.parametrize("dims", [(5, 7, 2), (13, 3, 4), (41, 70, 9), (70, 9, 41), (24, 12, 13)])
 def test_fp32_operator_shapes(P, dims, shape):
     from pytopo3d_b200._tensors import to_flat
@@ -112,6 +113,33 @@ def test_fp32_operator_shapes(P, dims, shape):
     assert s.stats()["fp64_fallback"] == 0
     s.close()
     r64.close()
+
+
+# The one-barrier kernel (FP32 shapes 6-7) does the two-barrier kernel's
+# arithmetic in the same order: its Apply output is bit-identical to the
+# two-barrier kernel's, whatever the tile, and its solves (every epilogue mode)
+# give the same compliance.
+@pytest.mark.parametrize("dims", [(5, 7, 2), (41, 70, 9), (70, 9, 41), (24, 12, 13)])
+def test_one_barrier_kernel_is_bit_identical(P, dims):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=3 * nx + nz, lo=0.05)
+    u = torch.as_tensor(np.random.default_rng(4).normal(size=fmask.size), dtype=torch.float32).cuda()
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    outs, comps = [], []
+    for shape in (5, 6, 7):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", fine_operator=3 + shape)
+        s.set_density(to_flat(rho), 3.0)
+        assert s.stats()["fine_form_fp32"] == 1 + shape
+        outs.append(s.apply(u).cpu())
+        comps.append(float(F @ s.solve(F)))
+        s.close()
+    for y, c in zip(outs[1:], comps[1:]):
+        assert torch.equal(y, outs[0])
+        assert c == pytest.approx(comps[0], rel=1e-9)
 
 
 @pytest.mark.parametrize("tag", ["8x4x4", "32x16x16"])
