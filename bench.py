@@ -519,8 +519,10 @@ def main():
                      "launch_ms": main_r["apply_ms"],
                      "executed_flops_per_node": flops_node,
                      "executed_tflops": flops_node * nnode / (main_r["apply_ms"] * 1e-3) / 1e12},
-        "roofline_coarse": {"bound": "hbm", "kernel": "stencil_apply_kernel (level 1, packed "
-                                                      + ("bf16" if fp32 else "fp64") + " stencil, cold L2)",
+        "roofline_coarse": {"bound": "hbm", "kernel": ("nm3_apply_kernel (level 1, node-major bf16 stencil, cold L2)"
+                                                      if fp32 and getattr(loop.solver.opts, "coarse_node_major", 0)
+                                                      else "stencil_apply_kernel (level 1, packed "
+                                                      + ("bf16" if fp32 else "fp64") + " stencil, cold L2)"),
                             "achieved": c_gbs, "peak": peak, "unit": "GB/s", "frac": c_gbs / peak,
                             "bytes_per_launch": c_bytes, "launch_ms": c_ms},
         "roofline_step": {"bound": "hbm", "what": "algorithmic bytes of the CG loop's kernels per step / step time",

@@ -258,6 +258,10 @@ typedef struct tp3d_solver_opts {
   int fine_slab_depth;  /* Walsh-Hadamard fine operator: node planes per block along z; 0 (default)
                            the fastest of the tile model's depth, half of it and twice it, timed with
                            the launch shapes; > 0 that depth only (profiling, reproducible tiles) */
+  int coarse_node_major; /* mixed form, 1 (default): bf16 coarse levels with more than split_dofs DOFs
+                           apply their stencil from a node-major copy (three lanes per node, one per
+                           z-plane of neighbours, 16-byte coefficient loads, each neighbour's u
+                           loaded once per node); 0: the packed layout, one thread per DOF */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -298,6 +302,12 @@ int tp3d_solver_solve_end(tp3d_solver* s, int* iterations, double* relres, int* 
 
 int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
 int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
+/* Coarse level `level` (1 .. levels - 2) of the mixed form's multigrid applied as
+ * the V-cycle applies it (bf16 or FP32 stencil, packed or node-major): y = A u on
+ * the level's free DOFs, y = u on its fixed DOFs; u, y: device FP32 vectors of
+ * 3 x the level's nodes.  Test helper for the coarse-level kernels; the
+ * reference's direct solve has no multigrid levels. */
+int tp3d_solver_apply_level_f32(tp3d_solver* s, int level, const float* u, float* y);
 
 /* Average device time (ms) of the fine-level operator kernel over `launches`
  * back-to-back launches on the solver's stream, timed with one pair of CUDA

@@ -27,6 +27,7 @@
 #include <tuple>
 #include <vector>
 
+#include "tp3d_coarse_nm.cuh"
 #include "tp3d_fine.cuh"
 #include "tp3d_fine_wht.cuh"
 #include "tp3d_coarse.cuh"
@@ -302,6 +303,7 @@ struct tp3d_solver {
   // conditional node (plain_next), so that every such launch follows a kernel.
   bool pdl = true, pdl_region = false, plain_next = true;
   std::vector<__nv_bfloat16*> S16;  // packed stencils in bf16 of levels 1 .. o.coarse_bf16 (mixed form), or null
+  std::vector<__nv_bfloat16*> SN3;  // node-major copies of S16 (coarse_node_major levels), or null
   long long branch_count = 0;
   cudaStream_t st_branch = nullptr;   // captures the reliable-update branch
   cudaStream_t st_side = nullptr;     // the coarsest inverse, concurrent with the power iterations
@@ -696,6 +698,17 @@ struct tp3d_solver {
     const bool split = ndof <= o.split_dofs;  // four lanes per DOF on the small levels
     count_bytes(op_bytes<T, MODE>(ndof, grids[L].nnode(), 81.0 * stencil_bytes<T>(L) * (double)ndof));
     if constexpr (sizeof(T) == 4) {
+      if (L < (int)SN3.size() && SN3[L]) {
+        StencilParams<float, __nv_bfloat16> p;
+        p.g = grids[L];
+        p.S = SN3[L];
+        p.fix = fix[L];
+        p.io = io;
+        const long long nn = grids[L].nnode();
+        launch(kPdlCoarse, nm3_apply_kernel<float, MODE>, dim3(grid_blocks((nn + 9) / 10, 8)), dim3(256), 0, p);
+        TP3D_CHECK_LAUNCH();
+        return TP3D_OK;
+      }
       if (L < (int)S16.size() && S16[L]) {
         StencilParams<float, __nv_bfloat16> p;
         p.g = grids[L];
@@ -1834,6 +1847,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->spectra_streams = 1;
   o->cluster_cycle = 1;
   o->fine_slab_depth = 0;
+  o->coarse_node_major = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1983,6 +1997,7 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   }
   s->A64.assign(s->nlev, nullptr);
   s->S16.assign(s->nlev, nullptr);
+  s->SN3.assign(s->nlev, nullptr);
   s->st_pow.assign(s->nlev, nullptr);
   s->ev_pow_in.assign(s->nlev, nullptr);
   s->ev_pow_out.assign(s->nlev, nullptr);
@@ -2017,6 +2032,9 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
                         !(s->cyc_L0 > 0 && L >= s->cyc_L0);
       if (bf16) s->S16[L] = s->alloc<__nv_bfloat16>(243 * nn);
       else if (L > 0) b.A = s->alloc<float>(243 * nn);
+      // levels above the four-lanes-per-DOF size apply their bf16 stencil node-major
+      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs)
+        s->SN3[L] = s->alloc<__nv_bfloat16>((size_t)kNM3Row * nn);
     }
   }
   s->cn = (int)(3 * s->grids.back().nnode());
@@ -2323,6 +2341,10 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->deep_SN);
       count_launch();
     }
+    if (s->SN3[L]) {
+      nm3_pack_kernel<<<s->grid_blocks(nn * kNM3Row), 256, 0, st>>>(gc, s->S16[L], s->SN3[L]);
+      count_launch();
+    }
     if (L == s->clu_L && s->clu_SN) {
       deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->clu_SN);
       count_launch();
@@ -2443,6 +2465,18 @@ extern "C" int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y) {
   io.u = u;
   io.out = y;
   if (int rc = s->fine<float, kModeApply>(io)) return rc;
+  return s->leave();
+}
+
+// Coarse level L's operator as the V-cycle applies it (mixed form, FP32
+// vectors of 3 x the level's nodes): y = A_L u on the free DOFs, u on fixed ones.
+extern "C" int tp3d_solver_apply_level_f32(tp3d_solver* s, int level, const float* u, float* y) {
+  if (!s || !u || !y || !s->have_density || !s->mixed || level < 1 || level >= s->nlev - 1) return TP3D_ERR_ARG;
+  if (int rc = s->enter()) return rc;
+  OpIO<float> io;
+  io.u = u;
+  io.out = y;
+  if (int rc = s->apply_level<float, kModeApply>(level, io)) return rc;
   return s->leave();
 }
 

@@ -145,6 +145,14 @@ class HexSolver:
         _lib.check(fn(self._h, u.data_ptr(), y.data_ptr()), "apply")
         return y
 
+    def apply_level(self, level: int, u: torch.Tensor) -> torch.Tensor:
+        """Coarse level ``level``'s operator as the mixed form's V-cycle applies it
+        (tp3d_solver_apply_level_f32); u: FP32, 3 x the level's nodes."""
+        y = torch.empty_like(u)
+        _lib.check(_lib.lib().tp3d_solver_apply_level_f32(self._h, int(level), u.data_ptr(), y.data_ptr()),
+                   "apply_level")
+        return y
+
     def stats(self) -> dict:
         buf = (C.c_double * 32)()
         n = _lib.lib().tp3d_solver_stats(self._h, buf, 32)

@@ -337,6 +337,50 @@ def test_cluster_cycle_matches_block_cycle(P, dims, used):
     np.testing.assert_allclose(Us[1], Us[0], rtol=0, atol=1e-5 * np.abs(Us[0]).max())
 
 
+# Coarse levels from the node-major bf16 stencil (three lanes per node) against
+# the packed bf16 stencil (one thread per DOF): the same coefficients summed in
+# another order, so each level's operator agrees to FP32 rounding, and the mixed
+# solves agree with each other and with FP64.  split_dofs=0 puts every bf16
+# level on the node-major path, odd sizes give ragged last warps.
+@pytest.mark.parametrize("dims", [(24, 12, 13), (41, 18, 22), (64, 32, 32)])
+def test_node_major_coarse_levels_match_packed(P, dims):
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = dims
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=nx + 2 * nz, lo=0.01)
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    solvers = [HexSolver(nx, ny, nz, KE, fmask, precision="mixed", split_dofs=0, coarse_node_major=nm)
+               for nm in (0, 1)]
+    for s in solvers:
+        s.set_density(to_flat(rho), 3.0)
+    nlev = int(solvers[0].stats()["levels"])
+    assert nlev >= 3
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    g = list(solvers[0].grid)
+    for L in range(1, nlev - 1):
+        g = [(v + 1) // 2 for v in g]
+        nn = (g[0] + 1) * (g[1] + 1) * (g[2] + 1)
+        u = torch.randn(3 * nn, device="cuda", generator=gen, dtype=torch.float32)
+        y0, y1 = (s.apply_level(L, u) for s in solvers)
+        assert torch.isfinite(y1).all()
+        tol = 2e-6 * float(y0.abs().max())
+        assert float((y1 - y0).abs().max()) <= tol, (L, float((y1 - y0).abs().max()), tol)
+    r64 = HexSolver(nx, ny, nz, KE, fmask, precision="fp64", rtol=1e-12)
+    r64.set_density(to_flat(rho), 3.0)
+    c64 = float(F @ r64.solve(F))
+    its = []
+    for s in solvers:
+        c = float(F @ s.solve(F))
+        its.append(s.last_iterations)
+        assert abs(c - c64) <= 1e-6 * abs(c64)
+        assert s.stats()["fp64_fallback"] == 0
+        s.close()
+    r64.close()
+    assert abs(its[0] - its[1]) <= max(1, 0.05 * its[0]), its
+
+
 # Residual and restriction in one launch on the small levels are the same
 # operations as the two launches, summed in another order: same iterations
 # (within one or 2%), same solution to rounding.
