@@ -16,9 +16,10 @@
 //    epilogue of DOF 3n + a: the warp's loads and stores of the epilogue are
 //    30 consecutive DOFs.
 // The coefficients are the packed layout's bf16 values (fixed rows and columns
-// and neighbours past the grid already zero), permuted by nm3_pack_kernel; the
-// rows are summed in a different order, so results round differently from the
-// packed kernel's.
+// and neighbours past the grid zero): the level builders write them node-major
+// directly (store_packed_rows), and levels built otherwise (the stencil triple
+// product) are permuted by nm3_pack_kernel.  The rows are summed in a
+// different order, so results round differently from the packed kernel's.
 #pragma once
 
 #include "tp3d_hex.cuh"
@@ -27,6 +28,12 @@ namespace tp3d {
 
 constexpr int kNM3Seg = 88;           // entries per z-plane segment (81 + 7 zeros)
 constexpr int kNM3Row = 3 * kNM3Seg;  // entries per node (528 bytes)
+
+// Entry of node n for the neighbour at z-plane a, x-offset b, y-offset e
+// (each 0..2, offset + 1), row component c and column component d.
+__host__ __device__ __forceinline__ long long nm3_index(long long n, int a, int b, int e, int c, int d) {
+  return n * kNM3Row + a * kNM3Seg + ((3 * b + e) * 3 + c) * 3 + d;
+}
 
 // Node-major copy of a level's packed bf16 stencil S (entry (n, c, j, d) at
 // S[(3 j + d) ndof + 3 n + c], j = 9 a + 3 b + e the neighbour in z, x, y order):

@@ -11,6 +11,7 @@
 // thread carries 27 accumulators.
 #pragma once
 
+#include "tp3d_coarse_nm.cuh"
 #include "tp3d_hex.cuh"
 
 namespace tp3d {
@@ -60,12 +61,14 @@ __device__ __forceinline__ void build_l1_rows(const Grid& gf, const Grid& gc, co
 }
 
 // The rows this thread built (node n, row component c, z-offset dzr), also
-// in the apply layout of stencil_pack_kernel: fixed rows / columns and
-// neighbours past the grid set to zero.
+// in the apply layout of stencil_pack_kernel (P, when given) and in the
+// node-major layout of nm3_apply_kernel (N, when given; its zero pad entries
+// are set once at allocation): fixed rows / columns and neighbours past the
+// grid set to zero.
 template <typename TP>
 __device__ __forceinline__ void store_packed_rows(const Grid& g, const uint8_t* __restrict__ fix, long long n, int ix,
                                                   int iy, int iz, int c, int dzr, const double (&acc)[9][3],
-                                                  TP* P) {
+                                                  TP* P, TP* N) {
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
   const long long ndof = 3 * g.nnode();
   const bool fi = (fix[n] >> c) & 1;
@@ -81,16 +84,18 @@ __device__ __forceinline__ void store_packed_rows(const Grid& g, const uint8_t* 
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const double v = (fi || ((fm >> d) & 1)) ? 0.0 : acc[(jx + 1) * 3 + (jy + 1)][d];
-        P[(long long)(jr * 3 + d) * ndof + 3 * n + c] = (TP)v;
+        if (P) P[(long long)(jr * 3 + d) * ndof + 3 * n + c] = (TP)v;
+        if (N) N[nm3_index(n, dzr + 1, jx + 1, jy + 1, c, d)] = (TP)v;
       }
     }
 }
 
-// With P given, also writes the apply layout (see store_packed_rows).
+// With P / N given, also writes the apply layouts (see store_packed_rows).
 template <typename TP>
 __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Grid gc, const double* __restrict__ E,
                                                                      const double* __restrict__ KE1, double* A,
-                                                                     const uint8_t* __restrict__ fixc, TP* P) {
+                                                                     const uint8_t* __restrict__ fixc, TP* P,
+                                                                     TP* N) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = gc.nnode();
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Gr
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
-  if (P) store_packed_rows<TP>(gc, fixc, n, Ix, Iy, Iz, c, dzr, acc, P);
+  if (P || N) store_packed_rows<TP>(gc, fixc, n, Ix, Iy, Iz, c, dzr, acc, P, N);
 }
 
 // ---- stencil Galerkin product A_c = P^T A_f P ----
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(576) elem_coarsen_kernel(Grid gf, Grid gc, con
 template <typename TP>
 __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid g, const double* __restrict__ Ke,
                                                                            double* A, const uint8_t* __restrict__ fix,
-                                                                           TP* P) {
+                                                                           TP* P, TP* N) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = g.nnode();
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid 
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
-  if (P) store_packed_rows<TP>(g, fix, n, ix, iy, iz, c, dzr, acc, P);
+  if (P || N) store_packed_rows<TP>(g, fix, n, ix, iy, iz, c, dzr, acc, P, N);
 }
 
 // ---- coarse fixed-DOF masks ----

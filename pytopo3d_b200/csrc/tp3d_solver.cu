@@ -2033,8 +2033,13 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       if (bf16) s->S16[L] = s->alloc<__nv_bfloat16>(243 * nn);
       else if (L > 0) b.A = s->alloc<float>(243 * nn);
       // levels above the four-lanes-per-DOF size apply their bf16 stencil node-major
-      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs)
+      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs) {
         s->SN3[L] = s->alloc<__nv_bfloat16>((size_t)kNM3Row * nn);
+        // pad entries stay zero; the builders write the others
+        if (s->SN3[L] && cudaMemsetAsync(s->SN3[L], 0, (size_t)kNM3Row * nn * sizeof(__nv_bfloat16), s->st) !=
+                             cudaSuccess)
+          return fail(TP3D_ERR_CUDA, "node-major stencil: memset failed");
+      }
     }
   }
   s->cn = (int)(3 * s->grids.back().nnode());
@@ -2289,7 +2294,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     const Grid& gc = s->grids[Lc];
     const long long nn = gc.nnode();
     stencil_from_elems_kernel<float><<<(unsigned)((nn + 31) / 32), kBuildThreads, 0, s->st_side>>>(
-        gc, s->Kel[Lc], s->A64[Lc], s->fix[Lc], nullptr);
+        gc, s->Kel[Lc], s->A64[Lc], s->fix[Lc], nullptr, nullptr);
     stencil_diag_inv_kernel<double><<<s->grid_blocks(nn), 256, 0, s->st_side>>>(gc, s->A64[Lc], s->fix[Lc],
                                                                                  s->L64[Lc].dinv);
     count_launch();
@@ -2306,16 +2311,19 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     // precision (bf16 where the level holds its stencil in bf16)
     float* P32 = mixed && !s->S16[L] ? s->L32[L].A : nullptr;
     double* P64 = mixed ? nullptr : s->L64[L].A;
-    __nv_bfloat16* P16 = s->S16[L];
+    // a level applied node-major needs its packed bf16 layout only for the
+    // fused residual-restriction kernel
+    __nv_bfloat16* N16 = s->SN3[L];
+    __nv_bfloat16* P16 = s->S16[L] && (!N16 || 3 * gc.nnode() <= s->o.resid_restrict_dofs) ? s->S16[L] : nullptr;
     bool packed = true;
     if (L == 1) {
-      if (P16) build_level1_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P16);
-      else if (mixed) build_level1_kernel<float><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P32);
-      else build_level1_kernel<double><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P64);
+      if (s->S16[L]) build_level1_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P16, N16);
+      else if (mixed) build_level1_kernel<float><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P32, nullptr);
+      else build_level1_kernel<double><<<nb, kBuildThreads, 0, st>>>(gf, gc, s->E64, s->KE1, s->A64[1], s->fix[1], P64, nullptr);
     } else if (s->o.galerkin == 0) {
-      if (P16) stencil_from_elems_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P16);
-      else if (mixed) stencil_from_elems_kernel<float><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P32);
-      else stencil_from_elems_kernel<double><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P64);
+      if (s->S16[L]) stencil_from_elems_kernel<__nv_bfloat16><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P16, N16);
+      else if (mixed) stencil_from_elems_kernel<float><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P32, nullptr);
+      else stencil_from_elems_kernel<double><<<nb, kBuildThreads, 0, st>>>(gc, s->Kel[L], s->A64[L], s->fix[L], P64, nullptr);
     } else {
       rap_kernel<<<nb, kBuildThreads, 0, st>>>(gf, gc, s->A64[L - 1], s->A64[L]);
       packed = false;
@@ -2327,8 +2335,9 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
     if (mixed) {
       convert_kernel<double, float><<<s->grid_blocks(3 * nn), 256, 0, st>>>(3 * nn, s->L64[L].dinv, s->L32[L].dinv);
       count_launch();
-      if (!packed && P16) {
-        stencil_pack_sym_kernel<__nv_bfloat16><<<s->grid_blocks(3 * nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L], P16);
+      if (!packed && s->S16[L]) {
+        stencil_pack_sym_kernel<__nv_bfloat16><<<s->grid_blocks(3 * nn), 256, 0, st>>>(gc, s->A64[L], s->fix[L],
+                                                                                      s->S16[L]);
         count_launch();
       } else if (!packed) {
         s->pack_level<float>(L, s->L32[L].A);
@@ -2341,7 +2350,7 @@ extern "C" int tp3d_solver_set_density(tp3d_solver* s, const double* rho, double
       deep_pack_kernel<<<s->grid_blocks(nn * kDeepRow), 256, 0, st>>>(gc, s->A64[L], s->fix[L], s->deep_SN);
       count_launch();
     }
-    if (s->SN3[L]) {
+    if (s->SN3[L] && !packed) {  // the builders write the node-major rows themselves
       nm3_pack_kernel<<<s->grid_blocks(nn * kNM3Row), 256, 0, st>>>(gc, s->S16[L], s->SN3[L]);
       count_launch();
     }

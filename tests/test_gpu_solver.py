@@ -341,9 +341,12 @@ def test_cluster_cycle_matches_block_cycle(P, dims, used):
 # the packed bf16 stencil (one thread per DOF): the same coefficients summed in
 # another order, so each level's operator agrees to FP32 rounding, and the mixed
 # solves agree with each other and with FP64.  split_dofs=0 puts every bf16
-# level on the node-major path, odd sizes give ragged last warps.
+# level on the node-major path, odd sizes give ragged last warps.  The level
+# builders write the node-major rows themselves (galerkin 0); the stencil triple
+# product (galerkin 1) is permuted from the packed layout.
+@pytest.mark.parametrize("galerkin", [0, 1])
 @pytest.mark.parametrize("dims", [(24, 12, 13), (41, 18, 22), (64, 32, 32)])
-def test_node_major_coarse_levels_match_packed(P, dims):
+def test_node_major_coarse_levels_match_packed(P, dims, galerkin):
     from pytopo3d_b200._tensors import to_flat
     from pytopo3d_b200.solver import HexSolver
 
@@ -351,8 +354,8 @@ def test_node_major_coarse_levels_match_packed(P, dims):
     KE = P.lk_H8(elem_size=1.0)
     rho, free, fmask = _problem(nx, ny, nz, seed=nx + 2 * nz, lo=0.01)
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
-    solvers = [HexSolver(nx, ny, nz, KE, fmask, precision="mixed", split_dofs=0, coarse_node_major=nm)
-               for nm in (0, 1)]
+    solvers = [HexSolver(nx, ny, nz, KE, fmask, precision="mixed", split_dofs=0, coarse_node_major=nm,
+                         galerkin=galerkin) for nm in (0, 1)]
     for s in solvers:
         s.set_density(to_flat(rho), 3.0)
     nlev = int(solvers[0].stats()["levels"])
