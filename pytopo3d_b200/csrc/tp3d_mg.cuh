@@ -60,34 +60,67 @@ __device__ __forceinline__ void build_l1_rows(const Grid& gf, const Grid& gc, co
   }
 }
 
+// The value of the apply layouts for entry (jx, jy, d) of the rows this thread
+// built (node n, row component c, z-plane iz + dzr): zero on fixed rows /
+// columns and for neighbours past the grid.
+__device__ __forceinline__ double masked_row_entry(const Grid& g, const uint8_t* __restrict__ fix, bool fixed_row,
+                                                   int ix, int iy, int z, int jx, int jy, int d,
+                                                   const double (&acc)[9][3]) {
+  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+  const int x = ix + jx, y = iy + jy;
+  const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
+  const int fm = in ? fix[g.nidx(x, y, z)] : 7;
+  return (fixed_row || ((fm >> d) & 1)) ? 0.0 : acc[(jx + 1) * 3 + (jy + 1)][d];
+}
+
 // The rows this thread built (node n, row component c, z-offset dzr), also
-// in the apply layout of stencil_pack_kernel (P, when given) and in the
-// node-major layout of nm3_apply_kernel (N, when given; its zero pad entries
-// are set once at allocation): fixed rows / columns and neighbours past the
-// grid set to zero.
+// in the apply layout of stencil_pack_kernel.
 template <typename TP>
 __device__ __forceinline__ void store_packed_rows(const Grid& g, const uint8_t* __restrict__ fix, long long n, int ix,
                                                   int iy, int iz, int c, int dzr, const double (&acc)[9][3],
-                                                  TP* P, TP* N) {
-  const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
+                                                  TP* P) {
   const long long ndof = 3 * g.nnode();
   const bool fi = (fix[n] >> c) & 1;
-  const int z = iz + dzr;
 #pragma unroll
   for (int jx = -1; jx <= 1; ++jx)
 #pragma unroll
     for (int jy = -1; jy <= 1; ++jy) {
-      const int x = ix + jx, y = iy + jy;
-      const bool in = x >= 0 && x < NX && y >= 0 && y < NY && z >= 0 && z < NZ;
-      const int fm = in ? fix[g.nidx(x, y, z)] : 7;
       const int jr = jrel_of(jx, jy, dzr);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double v = (fi || ((fm >> d) & 1)) ? 0.0 : acc[(jx + 1) * 3 + (jy + 1)][d];
-        if (P) P[(long long)(jr * 3 + d) * ndof + 3 * n + c] = (TP)v;
-        if (N) N[nm3_index(n, dzr + 1, jx + 1, jy + 1, c, d)] = (TP)v;
-      }
+      for (int d = 0; d < 3; ++d)
+        P[(long long)(jr * 3 + d) * ndof + 3 * n + c] =
+            (TP)masked_row_entry(g, fix, fi, ix, iy, iz + dzr, jx, jy, d, acc);
     }
+}
+
+// Node-major bf16 rows (nm3_apply_kernel's layout) of a builder block's 32
+// nodes n0 .. n0 + 31: every warp of the block (row component c, z-offset dzr)
+// puts its masked entries into a shared copy of the 32 rows (pad entries
+// zero), then the block writes the rows, which are contiguous in N, with
+// 16-byte stores.  Every thread of the block calls it.
+__device__ __forceinline__ void write_node_major_rows(const Grid& g, const uint8_t* __restrict__ fix, long long n0,
+                                                      bool live, int lane, int ix, int iy, int iz, int c, int dzr,
+                                                      const double (&acc)[9][3], __nv_bfloat16* N) {
+  __shared__ __align__(16) __nv_bfloat16 stage[32 * kNM3Row];
+  uint4* st4 = reinterpret_cast<uint4*>(stage);
+  constexpr int kChunksPerNode = kNM3Row * 2 / 16;  // 33
+  for (int i = threadIdx.x; i < 32 * kChunksPerNode; i += blockDim.x) st4[i] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  if (live) {
+    const bool fi = (fix[n0 + lane] >> c) & 1;
+#pragma unroll
+    for (int jx = -1; jx <= 1; ++jx)
+#pragma unroll
+      for (int jy = -1; jy <= 1; ++jy)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          stage[nm3_index(lane, dzr + 1, jx + 1, jy + 1, c, d)] =
+              __double2bfloat16(masked_row_entry(g, fix, fi, ix, iy, iz + dzr, jx, jy, d, acc));
+  }
+  __syncthreads();
+  const long long nvalid = min(32LL, g.nnode() - n0);
+  uint4* dst = reinterpret_cast<uint4*>(N + n0 * kNM3Row);
+  for (int i = threadIdx.x; i < nvalid * kChunksPerNode; i += blockDim.x) dst[i] = st4[i];
 }
 
 // With P / N given, also writes the apply layouts (see store_packed_rows).
@@ -99,8 +132,8 @@ __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Gr
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = gc.nnode();
-  const long long n = (long long)blockIdx.x * 32 + lane;
-  if (n >= nn) return;
+  const long long n0 = (long long)blockIdx.x * 32, n = n0 + lane;
+  const bool live = n < nn;  // no early return: the node-major writer takes block barriers
   const int CY = gc.ny + 1, CX = gc.nx + 1;
   const int Iy = (int)(n % CY);
   const long long r = n / CY;
@@ -110,17 +143,21 @@ __global__ void __launch_bounds__(kBuildThreads) build_level1_kernel(Grid gf, Gr
   for (int i = 0; i < 9; ++i)
 #pragma unroll
     for (int d = 0; d < 3; ++d) acc[i][d] = 0.0;
-  if (dzr == -1) build_l1_rows<-1>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
-  else if (dzr == 0) build_l1_rows<0>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
-  else build_l1_rows<1>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
+  if (live) {
+    if (dzr == -1) build_l1_rows<-1>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
+    else if (dzr == 0) build_l1_rows<0>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
+    else build_l1_rows<1>(gf, gc, E, KE1, Ix, Iy, Iz, c, acc);
 #pragma unroll
-  for (int jx = -1; jx <= 1; ++jx)
+    for (int jx = -1; jx <= 1; ++jx)
 #pragma unroll
-    for (int jy = -1; jy <= 1; ++jy)
+      for (int jy = -1; jy <= 1; ++jy)
 #pragma unroll
-      for (int d = 0; d < 3; ++d)
-        A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
-  if (P || N) store_packed_rows<TP>(gc, fixc, n, Ix, Iy, Iz, c, dzr, acc, P, N);
+        for (int d = 0; d < 3; ++d)
+          A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
+    if (P) store_packed_rows<TP>(gc, fixc, n, Ix, Iy, Iz, c, dzr, acc, P);
+  }
+  if constexpr (sizeof(TP) == 2)
+    if (N) write_node_major_rows(gc, fixc, n0, live, lane, Ix, Iy, Iz, c, dzr, acc, N);
 }
 
 // ---- stencil Galerkin product A_c = P^T A_f P ----
@@ -289,8 +326,8 @@ __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid 
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = w / 3, dzr = w % 3 - 1;
   const long long nn = g.nnode();
-  const long long n = (long long)blockIdx.x * 32 + lane;
-  if (n >= nn) return;
+  const long long n0 = (long long)blockIdx.x * 32, n = n0 + lane;
+  const bool live = n < nn;  // no early return: the node-major writer takes block barriers
   const int NY = g.ny + 1, NX = g.nx + 1;
   const int iy = (int)(n % NY);
   const long long r = n / NY;
@@ -300,39 +337,43 @@ __global__ void __launch_bounds__(kBuildThreads) stencil_from_elems_kernel(Grid 
   for (int i = 0; i < 9; ++i)
 #pragma unroll
     for (int d = 0; d < 3; ++d) acc[i][d] = 0.0;
+  if (live) {
 #pragma unroll
-  for (int ez = -1; ez <= 0; ++ez) {
-    const int zc = iz + ez;
-    if (zc < 0 || zc >= g.nz) continue;
+    for (int ez = -1; ez <= 0; ++ez) {
+      const int zc = iz + ez;
+      if (zc < 0 || zc >= g.nz) continue;
 #pragma unroll
-    for (int ex = -1; ex <= 0; ++ex) {
-      const int xc = ix + ex;
-      if (xc < 0 || xc >= g.nx) continue;
+      for (int ex = -1; ex <= 0; ++ex) {
+        const int xc = ix + ex;
+        if (xc < 0 || xc >= g.nx) continue;
 #pragma unroll
-      for (int ey = -1; ey <= 0; ++ey) {
-        const int yc = iy + ey;
-        if (yc < 0 || yc >= g.ny) continue;
-        const int a = corner_index(-ex, -ey, -ez);
-        const double* rowp = Ke + (size_t)g.eidx(xc, yc, zc) * 576 + (3 * a + c) * 24;
+        for (int ey = -1; ey <= 0; ++ey) {
+          const int yc = iy + ey;
+          if (yc < 0 || yc >= g.ny) continue;
+          const int a = corner_index(-ex, -ey, -ez);
+          const double* rowp = Ke + (size_t)g.eidx(xc, yc, zc) * 576 + (3 * a + c) * 24;
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          if (ez + corner_oz(b) != dzr) continue;
-          const int jx = ex + corner_ox(b), jy = ey + corner_oy(b);
-          const int slot = (jx + 1) * 3 + (jy + 1);
+          for (int b = 0; b < 8; ++b) {
+            if (ez + corner_oz(b) != dzr) continue;
+            const int jx = ex + corner_ox(b), jy = ey + corner_oy(b);
+            const int slot = (jx + 1) * 3 + (jy + 1);
 #pragma unroll
-          for (int d = 0; d < 3; ++d) acc[slot][d] += __ldg(&rowp[3 * b + d]);
+            for (int d = 0; d < 3; ++d) acc[slot][d] += __ldg(&rowp[3 * b + d]);
+          }
         }
       }
     }
+#pragma unroll
+    for (int jx = -1; jx <= 1; ++jx)
+#pragma unroll
+      for (int jy = -1; jy <= 1; ++jy)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
+    if (P) store_packed_rows<TP>(g, fix, n, ix, iy, iz, c, dzr, acc, P);
   }
-#pragma unroll
-  for (int jx = -1; jx <= 1; ++jx)
-#pragma unroll
-    for (int jy = -1; jy <= 1; ++jy)
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        A[(long long)stencil_k(jrel_of(jx, jy, dzr), c, d) * nn + n] = acc[(jx + 1) * 3 + (jy + 1)][d];
-  if (P || N) store_packed_rows<TP>(g, fix, n, ix, iy, iz, c, dzr, acc, P, N);
+  if constexpr (sizeof(TP) == 2)
+    if (N) write_node_major_rows(g, fix, n0, live, lane, ix, iy, iz, c, dzr, acc, N);
 }
 
 // ---- coarse fixed-DOF masks ----

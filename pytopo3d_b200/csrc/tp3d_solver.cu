@@ -2033,13 +2033,8 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
       if (bf16) s->S16[L] = s->alloc<__nv_bfloat16>(243 * nn);
       else if (L > 0) b.A = s->alloc<float>(243 * nn);
       // levels above the four-lanes-per-DOF size apply their bf16 stencil node-major
-      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs) {
+      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs)
         s->SN3[L] = s->alloc<__nv_bfloat16>((size_t)kNM3Row * nn);
-        // pad entries stay zero; the builders write the others
-        if (s->SN3[L] && cudaMemsetAsync(s->SN3[L], 0, (size_t)kNM3Row * nn * sizeof(__nv_bfloat16), s->st) !=
-                             cudaSuccess)
-          return fail(TP3D_ERR_CUDA, "node-major stencil: memset failed");
-      }
     }
   }
   s->cn = (int)(3 * s->grids.back().nnode());
