@@ -62,3 +62,29 @@ def test_bad_arguments_are_rejected_on_the_host(libpath):
                             1e-8, None, None, None, None, None) == _lib.TP3D_ERR_ARG
     with pytest.raises(ValueError):
         _lib.check(_lib.TP3D_ERR_ARG, "x")
+
+
+@pytest.mark.parametrize("cname,pyname", [("tp3d_solver_opts", "SolverOpts"), ("tp3d_stage_desc", "StageDesc")])
+def test_ctypes_structs_mirror_the_header(tmp_path, cname, pyname):
+    """The Python mirror of each struct the header passes by pointer has the C
+    layout: a C program built with the header prints every field's offset and
+    the struct's size, and ctypes must agree on each of them."""
+    import shutil
+    import subprocess
+
+    from pytopo3d_b200 import _lib
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirror = getattr(_lib, pyname)
+    lines = [f'printf("%zu\\n", sizeof({cname}));']
+    lines += [f'printf("%zu\\n", offsetof({cname}, {n}));' for n, _ in mirror._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"topo3d_b200.h\"\n"
+                   "int main(void) {\n" + "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(mirror)
+    assert got[1:] == [getattr(mirror, n).offset for n, _ in mirror._fields_]
