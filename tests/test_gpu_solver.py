@@ -117,8 +117,8 @@ def test_fp32_operator_shapes(P, dims, shape):
 
 # The one-barrier kernel (FP32 shapes 6-7) does the two-barrier kernel's
 # arithmetic in the same order: its Apply output is bit-identical to the
-# two-barrier kernel's, whatever the tile, and its solves (every epilogue mode)
-# give the same compliance.
+# two-barrier kernel's, whatever the tile or slab depth, and its solves (every
+# epilogue mode) give the same compliance.
 @pytest.mark.parametrize("dims", [(5, 7, 2), (41, 70, 9), (70, 9, 41), (24, 12, 13)])
 def test_one_barrier_kernel_is_bit_identical(P, dims):
     from pytopo3d_b200._tensors import to_flat
@@ -134,6 +134,14 @@ def test_one_barrier_kernel_is_bit_identical(P, dims):
         s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", fine_operator=3 + shape)
         s.set_density(to_flat(rho), 3.0)
         assert s.stats()["fine_form_fp32"] == 1 + shape
+        outs.append(s.apply(u).cpu())
+        comps.append(float(F @ s.solve(F)))
+        s.close()
+    # a pinned slab depth (node planes per block) changes the tiling, not the result
+    for depth in (1, 3):
+        s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", fine_operator=9, fine_slab_depth=depth)
+        s.set_density(to_flat(rho), 3.0)
+        assert s.stats()["fine_slab_depth"] == min(depth, nz + 1)
         outs.append(s.apply(u).cpu())
         comps.append(float(F @ s.solve(F)))
         s.close()
