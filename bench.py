@@ -549,6 +549,11 @@ def run_batch(args):
     design after --warmup.  The same designs one after another on the default
     stream are timed beside it.  Prints one JSON line (not the headline bench
     line)."""
+    # the designs' streams run side by side only over as many hardware queues as
+    # the context has (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default): 32 measured
+    # 174 SIMP it/s against 144-150 for the stream runner (the graph runner is
+    # unaffected); read when the context is created, so set before any CUDA call
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import torch
 
     from pytopo3d_b200.batch import BatchRunner, batched_cantilevers

@@ -106,7 +106,12 @@ class BatchRunner:
     ("bytes", the default, or "time"; None: off) every design first runs three
     loop bodies alone, the third of which autotunes its smoothing degrees on its
     own grid (``HexSolver.autotune``).  The designs then share the GPU, where
-    throughput counts, so the default criterion is the solve's traffic."""
+    throughput counts, so the default criterion is the solve's traffic.
+
+    The designs' streams run concurrently only over as many hardware queues as
+    the CUDA context has: set ``CUDA_DEVICE_MAX_CONNECTIONS=32`` in the
+    environment before the process's first CUDA call (the default 8 cost about
+    15% on the 64-design workload; ``run_graph`` does not depend on it)."""
 
     def __init__(self, specs: List[DesignSpec], precision: str = "mixed", beta: float = 1.0, eta: float = 0.5,
                  move: float = 0.2, workers: int = 8, solver_options: Optional[dict] = None,
