@@ -199,7 +199,8 @@ typedef struct tp3d_solver_opts {
   double reliable_delta;/* mixed: replace the FP32 residual by the FP64 one when it fell by this factor */
   int max_restarts;     /* FP64: restarts from the true residual when the recursive one drifted */
   int fine_operator;    /* fine-level K u: 0 the fastest of the dense-KE form and the Walsh-Hadamard
-                           block form's launch shapes and slab depths, timed on the grid at the first
+                           block form's launch shapes, tile shapes (the three with the fewest blocks
+                           per node plane) and slab depths, timed on the grid at the first
                            set_density; 1 dense KE; 2 Walsh-Hadamard (fastest shape); 3 + v the
                            Walsh-Hadamard form with shape v only (FP64: v = 0..2; FP32: v = 0..2 the
                            packed two-plane kernel with paired FP32 instructions, 3..5 the scalar
@@ -358,8 +359,9 @@ int tp3d_solver_time_level(tp3d_solver* s, int level, int fp32, int launches, do
  * reliable-update branch excluded; 0 before the first solve), the kernels launched per CG
  * iteration, the autotuner state (0 not tuned, 1 searched, 2 from the cache), the smoothing degrees
  * of the fine level, level 1 and level 2, the fine operator's slab depth (node planes per block; 0
- * for the dense form) and threads per block of the Walsh-Hadamard form in use.  Returns the count
- * written. */
+ * for the dense form) and threads per block of the Walsh-Hadamard form in use, the first level of
+ * the cluster cycle (0 none) and its CTAs, and the Walsh-Hadamard form's interior tile (nodes along
+ * y, nodes along x; 0 for the dense form).  Returns the count written. */
 int tp3d_solver_stats(tp3d_solver* s, double* out, int n);
 
 /* ---------------------------------------------------------------------------

@@ -3,6 +3,7 @@
 // block shape; the KE block split; the tile chooser.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "tp3d_fine_wht.cuh"
 #include "tp3d_fine_wht1.cuh"
@@ -184,50 +185,70 @@ bool wht_blocks_from_ke(const double* KE, double m[8][3][3]) {
 }
 
 // The patch is PY = TY + 2 threads along y (the contiguous direction) by
-// TX + 2 along x; the tile with the fewest blocks per node plane wins (ties:
-// the larger tile).  Then the number of z chunks that minimises the busiest
-// SM's work, counting each block's prologue as 1.5 planes and crediting
-// co-resident blocks for hiding each other's barrier and memory latency.
+// TX + 2 along x.  Tile candidates are ranked by blocks per node plane (the
+// fewest first: the fewest halo threads), ties by the larger tile; each gets
+// the number of z chunks that minimises the busiest SM's work, counting each
+// block's prologue as 1.5 planes and crediting co-resident blocks for hiding
+// each other's barrier and memory latency.
 template <typename T, class ESrc>
-WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
+int wht_tile_candidates(const Grid& g, int nsm, int v, WhtTile* out, int max_out) {
   const int NX = g.nx + 1, NY = g.ny + 1, NZ = g.nz + 1;
-  WhtTile best;
-  best.variant = v;
-  best.nthr = WhtShapes<T>::nthr[v];
-  long long best_blocks = -1;
-  for (int PY = 4; PY <= std::min(best.nthr / 4, NY + 2); ++PY) {
-    const int TY = PY - 2;
-    const int TX = best.nthr / PY - 2;
+  const int nthr = WhtShapes<T>::nthr[v];
+  const int occ = wht_occupancy<T, ESrc>(v);
+  struct Cand {
+    long long blocks;
+    int area, PY;
+  };
+  std::vector<Cand> cands;
+  for (int PY = 4; PY <= std::min(nthr / 4, NY + 2); ++PY) {
+    const int TY = PY - 2, TX = nthr / PY - 2;
     if (TX < 2) continue;
-    const long long ky = (NY + TY - 1) / TY, kx = (NX + TX - 1) / TX;
-    const long long blocks = ky * kx;
-    if (best_blocks < 0 || blocks < best_blocks || (blocks == best_blocks && TX * TY > best.TX * best.TY)) {
-      best_blocks = blocks;
-      best.TX = TX;
-      best.TY = TY;
-      best.PY = PY;
-      best.tiles_y = (int)ky;
-      best.tiles_x = (int)kx;
-    }
+    const long long blocks = (long long)((NY + TY - 1) / TY) * ((NX + TX - 1) / TX);
+    cands.push_back({blocks, TX * TY, PY});
   }
-  best.occ = wht_occupancy<T, ESrc>(v);
+  std::sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) {
+    return x.blocks != y.blocks ? x.blocks < y.blocks : (x.area != y.area ? x.area > y.area : x.PY < y.PY);
+  });
   auto eff = [&](long long L) {
-    const long long l = std::min<long long>(L, best.occ);
+    const long long l = std::min<long long>(L, occ);
     return l <= 1 ? 1.0 : (l == 2 ? 1.6 : (l == 3 ? 1.85 : 2.0));
   };
-  double best_t = 1e300;
-  for (int zc = 1; zc <= NZ; ++zc) {
-    const long long nch = (NZ + zc - 1) / zc;
-    if ((nch - 1) * zc >= NZ) continue;
-    const long long per_sm = (best_blocks * nch + nsm - 1) / nsm;
-    const double t = (double)per_sm * (zc + 1.5) / eff(per_sm);
-    if (t < best_t - 1e-9) {
-      best_t = t;
-      best.ZC = zc;
-      best.zchunks = (int)nch;
+  int n = 0;
+  for (const Cand& c : cands) {
+    if (n >= max_out) break;
+    WhtTile t;
+    t.variant = v;
+    t.nthr = nthr;
+    t.occ = occ;
+    t.PY = c.PY;
+    t.TY = c.PY - 2;
+    t.TX = nthr / c.PY - 2;
+    t.tiles_y = (NY + t.TY - 1) / t.TY;
+    t.tiles_x = (NX + t.TX - 1) / t.TX;
+    double best_t = 1e300;
+    for (int zc = 1; zc <= NZ; ++zc) {
+      const long long nch = (NZ + zc - 1) / zc;
+      if ((nch - 1) * zc >= NZ) continue;
+      const long long per_sm = (c.blocks * nch + nsm - 1) / nsm;
+      const double tm = (double)per_sm * (zc + 1.5) / eff(per_sm);
+      if (tm < best_t - 1e-9) {
+        best_t = tm;
+        t.ZC = zc;
+        t.zchunks = (int)nch;
+      }
     }
+    out[n++] = t;
   }
-  return best;
+  return n;
+}
+
+template <typename T, class ESrc>
+WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
+  WhtTile t;
+  t.variant = v;
+  t.nthr = WhtShapes<T>::nthr[v];
+  wht_tile_candidates<T, ESrc>(g, nsm, v, &t, 1);
+  return t;
 }
 
 #define TP3D_WHT_INSTANTIATE(T, ESrc)                                                     \
@@ -236,7 +257,8 @@ WhtTile wht_choose_tile(const Grid& g, int nsm, int v) {
   template bool wht_variant_timed<T, ESrc>(int);                                         \
   template int wht_occupancy<T, ESrc>(int);                                              \
   template int wht_launch<T, ESrc>(const WhtParams<T, ESrc>&, int, int, dim3, cudaStream_t, bool); \
-  template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);
+  template WhtTile wht_choose_tile<T, ESrc>(const Grid&, int, int);                     \
+  template int wht_tile_candidates<T, ESrc>(const Grid&, int, int, WhtTile*, int);
 TP3D_WHT_INSTANTIATE(double, EFromF64)
 TP3D_WHT_INSTANTIATE(float, EFromF32)
 TP3D_WHT_INSTANTIATE(float, EFromBF16)

@@ -277,8 +277,13 @@ int wht_launch(const WhtParams<T, ESrc>& p, int mode, int v, dim3 grid, cudaStre
 // translation rows are not zero, in which case the dense form is used.
 bool wht_blocks_from_ke(const double* KE, double m[8][3][3]);
 
-// Tile and z chunking for variant v on grid g (nsm SMs).
+// Tile and z chunking for variant v on grid g (nsm SMs): the first of
+// wht_tile_candidates.
 template <typename T, class ESrc>
 WhtTile wht_choose_tile(const Grid& g, int nsm, int v);
+// Up to max_out tile shapes for variant v, the fewest blocks per node plane
+// first, each with its modelled z chunking; returns how many were written.
+template <typename T, class ESrc>
+int wht_tile_candidates(const Grid& g, int nsm, int v, WhtTile* out, int max_out);
 
 }  // namespace tp3d

@@ -68,6 +68,7 @@ double op_bytes(long long n, long long nn, double src) {
 }
 
 constexpr int kMaxPartials = 1 << 16;
+constexpr int kWhtTileCandidates = 3;  // tile shapes per Walsh-Hadamard launch shape in the timed choice
 constexpr int kSpectraPartials = 4096;  // per level at set-up: two reductions of at most 2048 blocks
 constexpr int kPdlCoarse = 1, kPdlFine = 2;  // tp3d_solver_opts::pdl bits
 
@@ -612,6 +613,12 @@ struct tp3d_solver {
     else return wht_choose_tile<float, EFromF32>(g, nsm, v);
   }
   template <typename T>
+  int wht_tiles_for(int v, WhtTile* out, int max_out) const {
+    if constexpr (sizeof(T) == 8) return wht_tile_candidates<double, EFromF64>(g, nsm, v, out, max_out);
+    else if (rho16) return wht_tile_candidates<float, EFromBF16>(g, nsm, v, out, max_out);
+    else return wht_tile_candidates<float, EFromF32>(g, nsm, v, out, max_out);
+  }
+  template <typename T>
   int choose_fine_form() {
     bool& use = sizeof(T) == 8 ? use_wht64 : use_wht32;
     WhtTile& wt = sizeof(T) == 8 ? wt64 : wt32;
@@ -646,25 +653,31 @@ struct tp3d_solver {
       if constexpr (sizeof(T) == 8) timed = wht_variant_timed<double, EFromF64>(v);
       else timed = wht_variant_timed<float, EFromF32>(v);
       if (o.fine_operator <= 2 && !timed) continue;
-      const WhtTile base = wht_tile_for<T>(v);
-      int zcs[3] = {base.ZC, std::max(1, base.ZC / 2), std::min(NZ, 2 * base.ZC)};
-      const int nzc = o.fine_slab_depth > 0 ? 1 : 3;
-      if (o.fine_slab_depth > 0) zcs[0] = std::min(NZ, o.fine_slab_depth);
-      for (int k = 0; k < nzc && rc == TP3D_OK; ++k) {
-        if (k > 0 && (zcs[k] == base.ZC || (k == 2 && zcs[2] == zcs[1]))) continue;
-        WhtTile w = base;
-        w.ZC = zcs[k];
-        w.zchunks = (NZ + w.ZC - 1) / w.ZC;
-        if ((long long)w.tiles_y * w.tiles_x * w.zchunks > kMaxPartials) continue;
-        wt = w;
-        use = true;
-        double ms = 0.0;
-        rc = time_one(&ms);
-        use = false;
-        if (rc == TP3D_OK && ms < best) {
-          best = ms;
-          best_t = w;
-          best_wht = true;
+      // the tile shapes with the fewest blocks per node plane (elements per
+      // block), each at its modelled slab depth, half and twice it
+      WhtTile tiles[kWhtTileCandidates];
+      const int ntile = wht_tiles_for<T>(v, tiles, kWhtTileCandidates);
+      for (int ti = 0; ti < ntile && rc == TP3D_OK; ++ti) {
+        const WhtTile& base = tiles[ti];
+        int zcs[3] = {base.ZC, std::max(1, base.ZC / 2), std::min(NZ, 2 * base.ZC)};
+        const int nzc = o.fine_slab_depth > 0 ? 1 : 3;
+        if (o.fine_slab_depth > 0) zcs[0] = std::min(NZ, o.fine_slab_depth);
+        for (int k = 0; k < nzc && rc == TP3D_OK; ++k) {
+          if (k > 0 && (zcs[k] == base.ZC || (k == 2 && zcs[2] == zcs[1]))) continue;
+          WhtTile w = base;
+          w.ZC = zcs[k];
+          w.zchunks = (NZ + w.ZC - 1) / w.ZC;
+          if ((long long)w.tiles_y * w.tiles_x * w.zchunks > kMaxPartials) continue;
+          wt = w;
+          use = true;
+          double ms = 0.0;
+          rc = time_one(&ms);
+          use = false;
+          if (rc == TP3D_OK && ms < best) {
+            best = ms;
+            best_t = w;
+            best_wht = true;
+          }
         }
       }
     }
@@ -2681,7 +2694,9 @@ extern "C" int tp3d_solver_stats(tp3d_solver* s, double* out, int n) {
                            (double)s->pre_sweeps(2),
                            (double)(s->mixed ? (s->use_wht32 ? s->wt32.ZC : 0) : (s->use_wht64 ? s->wt64.ZC : 0)),
                            (double)(s->mixed ? (s->use_wht32 ? s->wt32.nthr : 0) : (s->use_wht64 ? s->wt64.nthr : 0)),
-                           (double)s->clu_L, (double)s->clu_C};
+                           (double)s->clu_L, (double)s->clu_C,
+                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.TY : 0) : (s->use_wht64 ? s->wt64.TY : 0)),
+                           (double)(s->mixed ? (s->use_wht32 ? s->wt32.TX : 0) : (s->use_wht64 ? s->wt64.TX : 0))};
   const int m = std::min<int>(n, (int)v.size());
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;

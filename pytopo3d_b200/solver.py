@@ -154,14 +154,14 @@ class HexSolver:
         return y
 
     def stats(self) -> dict:
-        buf = (C.c_double * 32)()
-        n = _lib.lib().tp3d_solver_stats(self._h, buf, 32)
+        buf = (C.c_double * 40)()
+        n = _lib.lib().tp3d_solver_stats(self._h, buf, 40)
         keys = ["levels", "iterations", "reliable_updates", "relres", "restarts", "coarsest_dofs",
                 "tile_y", "tile_x", "z_chunk", "coarse_fallback", "lambda_max_fine", "residual_floor",
                 "fp64_fallback", "fine_form_fp64", "fine_form_fp32", "fused_cycle_level", "device_loop",
                 "pdl", "coarse_bf16", "coarsest_status", "deep_cta_level", "bytes_per_cg_iteration",
                 "kernels_per_cg_iteration", "autotuned", "degree_fine", "degree_level1", "degree_level2",
-                "fine_slab_depth", "fine_threads", "cluster_level", "cluster_ctas"]
+                "fine_slab_depth", "fine_threads", "cluster_level", "cluster_ctas", "fine_tile_y", "fine_tile_x"]
         return {k: buf[i] for i, k in enumerate(keys[:n])}
 
     def autotune(self, F: torch.Tensor, U0: Optional[torch.Tensor] = None, criterion: Optional[str] = None) -> dict:

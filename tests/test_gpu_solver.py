@@ -133,7 +133,11 @@ def test_one_barrier_kernel_is_bit_identical(P, dims):
     for shape in (5, 6, 7):
         s = HexSolver(nx, ny, nz, KE, fmask, precision="mixed", fine_operator=3 + shape)
         s.set_density(to_flat(rho), 3.0)
-        assert s.stats()["fine_form_fp32"] == 1 + shape
+        st = s.stats()
+        assert st["fine_form_fp32"] == 1 + shape
+        # the tile the timed choice kept covers the grid with whole node rows
+        assert 2 <= st["fine_tile_y"] and 2 <= st["fine_tile_x"]
+        assert (st["fine_tile_y"] + 2) * (st["fine_tile_x"] + 2) <= st["fine_threads"]
         outs.append(s.apply(u).cpu())
         comps.append(float(F @ s.solve(F)))
         s.close()
