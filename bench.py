@@ -329,7 +329,7 @@ def main():
     ap.add_argument("--fine-operator", type=int, default=0,
                     help="solver option fine_operator for --mode step/apply (0 timed choice)")
     ap.add_argument("--solver-opt", action="append", default=[], metavar="KEY=VALUE",
-                    help="further solver options for --mode step/apply (integers or floats)")
+                    help="further solver options for --mode step/apply/batch (integers or floats)")
     args = ap.parse_args()
     if args.mode == "batch":
         return run_batch(args)
@@ -560,10 +560,11 @@ def run_batch(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     specs = batched_cantilevers(64, seed=0)
+    opts = solver_opts_of(args)
     tuned = {}
     for crit in ("bytes", "time"):
         t0 = time.perf_counter()
-        br = BatchRunner(specs, precision=args.precision, workers=8, tune=crit)
+        br = BatchRunner(specs, precision=args.precision, workers=8, tune=crit, solver_options=opts)
         setup_s = time.perf_counter() - t0
         br.run(max(1, args.warmup))
         r = br.run(args.steps)
@@ -573,16 +574,16 @@ def run_batch(args):
         br.close()
     # the same position on each design's trajectory as the tuned runs (three
     # loop bodies of tuning plus the warm-up)
-    br = BatchRunner(specs, precision=args.precision, workers=8, tune=None)
+    br = BatchRunner(specs, precision=args.precision, workers=8, tune=None, solver_options=opts)
     br.run(3 + max(1, args.warmup))
     conc_default = br.run(args.steps)
     br.close()
     # every design advanced by one graph launch per call (no host thread per design)
-    br = BatchRunner(specs, precision=args.precision, workers=8, tune="bytes")
+    br = BatchRunner(specs, precision=args.precision, workers=8, tune="bytes", solver_options=opts)
     br.run_graph(max(1, args.warmup))
     graph_tuned = br.run_graph(args.steps)
     br.close()
-    seq = BatchRunner(specs, precision=args.precision, workers=1, tune=None)
+    seq = BatchRunner(specs, precision=args.precision, workers=1, tune=None, solver_options=opts)
     seq.run(3 + max(1, args.warmup))
     one = seq.run(args.steps)
     seq.close()
@@ -666,6 +667,15 @@ def run_large(args):
     return 0
 
 
+def solver_opts_of(args):
+    """Solver options given as --solver-opt KEY=VALUE (integers or floats)."""
+    opts = {}
+    for kv in args.solver_opt:
+        k, v = kv.split("=", 1)
+        opts[k] = float(v) if any(ch in v for ch in ".e") else int(v)
+    return opts
+
+
 def run_probe(args):
     """Small fixed workloads for profiler captures (no timing printed as a bench value)."""
     global NELX, NELY, NELZ
@@ -673,10 +683,7 @@ def run_probe(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     NELX, NELY, NELZ = args.size, args.size // 2, args.size // 2
-    opts = {"fine_operator": args.fine_operator}
-    for kv in args.solver_opt:
-        k, v = kv.split("=", 1)
-        opts[k] = float(v) if any(ch in v for ch in ".e") else int(v)
+    opts = {"fine_operator": args.fine_operator, **solver_opts_of(args)}
     loop = make_loop(args.precision, solver_options=opts)
     if args.mode == "step":
         for _ in range(max(1, args.warmup)):

@@ -235,8 +235,9 @@ typedef struct tp3d_solver_opts {
                            FP64 residuals are unchanged, so the stopping test is too.  Used with
                            the Chebyshev smoother, whose interval is measured on the operator it
                            smooths (damped Jacobi's fixed omega has no margin for the rounding). */
-  int split_dofs;       /* coarse levels with at most this many DOFs apply their stencil with four
-                           threads per DOF (more loads in flight on levels too small to fill the
+  int split_dofs;       /* packed-layout coarse levels (the FP64 form, FP32 levels, bf16 levels with
+                           coarse_node_major = 0) with at most this many DOFs apply their stencil with
+                           four threads per DOF (more loads in flight on levels too small to fill the
                            GPU); larger levels one thread per DOF */
   int deep_cta;         /* mixed form, 1 (default): the last smoothed level and the coarsest solve run
                            as one thread block with the level's operator in shared memory (when it
@@ -259,10 +260,11 @@ typedef struct tp3d_solver_opts {
   int fine_slab_depth;  /* Walsh-Hadamard fine operator: node planes per block along z; 0 (default)
                            the fastest of the tile model's depth, half of it and twice it, timed with
                            the launch shapes; > 0 that depth only (profiling, reproducible tiles) */
-  int coarse_node_major; /* mixed form, 1 (default): bf16 coarse levels with more than split_dofs DOFs
-                           apply their stencil from a node-major copy (three lanes per node, one per
-                           z-plane of neighbours, 16-byte coefficient loads, each neighbour's u
-                           loaded once per node); 0: the packed layout, one thread per DOF */
+  int coarse_node_major; /* mixed form, 1 (default): the bf16 coarse levels apply their stencil from a
+                           node-major copy (three lanes per node, one per z-plane of neighbours,
+                           16-byte coefficient loads, each neighbour's u loaded once per node);
+                           0: the packed layout (split_dofs decides between one thread and four
+                           lanes per DOF) */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);

@@ -2045,9 +2045,9 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
                         !(s->cyc_L0 > 0 && L >= s->cyc_L0);
       if (bf16) s->S16[L] = s->alloc<__nv_bfloat16>(243 * nn);
       else if (L > 0) b.A = s->alloc<float>(243 * nn);
-      // levels above the four-lanes-per-DOF size apply their bf16 stencil node-major
-      if (bf16 && s->o.coarse_node_major && ndof > s->o.split_dofs)
-        s->SN3[L] = s->alloc<__nv_bfloat16>((size_t)kNM3Row * nn);
+      // bf16 levels apply their stencil node-major (the cluster or block cycle's
+      // levels run from their own node-major rows in shared memory)
+      if (bf16 && s->o.coarse_node_major) s->SN3[L] = s->alloc<__nv_bfloat16>((size_t)kNM3Row * nn);
     }
   }
   s->cn = (int)(3 * s->grids.back().nnode());

@@ -269,7 +269,8 @@ def test_split_stencil_matches_one_thread_per_dof(P, dims, prec):
     F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
     its, Us = [], []
     for split in (0, 1 << 30):
-        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, split_dofs=split, fine_operator=3)
+        s = HexSolver(nx, ny, nz, KE, fmask, precision=prec, split_dofs=split, fine_operator=3,
+                      coarse_node_major=0)
         s.set_density(to_flat(rho), 3.0)
         U = s.solve(F)
         its.append(s.last_iterations)
@@ -352,8 +353,8 @@ def test_cluster_cycle_matches_block_cycle(P, dims, used):
 # Coarse levels from the node-major bf16 stencil (three lanes per node) against
 # the packed bf16 stencil (one thread per DOF): the same coefficients summed in
 # another order, so each level's operator agrees to FP32 rounding, and the mixed
-# solves agree with each other and with FP64.  split_dofs=0 puts every bf16
-# level on the node-major path, odd sizes give ragged last warps.  The level
+# solves agree with each other and with FP64.  split_dofs=0 keeps the packed
+# solver's small levels at one thread per DOF; odd sizes give ragged last warps.  The level
 # builders write the node-major rows themselves (galerkin 0); the stencil triple
 # product (galerkin 1) is permuted from the packed layout.
 @pytest.mark.parametrize("galerkin", [0, 1])
