@@ -265,6 +265,9 @@ typedef struct tp3d_solver_opts {
                            16-byte coefficient loads, each neighbour's u loaded once per node);
                            0: the packed layout (split_dofs decides between one thread and four
                            lanes per DOF) */
+  int ritz_start;       /* 1 (default): keep the buffers of tp3d_solver_ritz_start, and start each
+                           solve of a stage graph from the Rayleigh-Ritz combination of the last two
+                           solutions; 0: the linear extrapolation of tp3d_warm_start */
 } tp3d_solver_opts;
 
 void tp3d_solver_default_opts(tp3d_solver_opts* opts);
@@ -303,6 +306,17 @@ int tp3d_solver_solve(tp3d_solver* s, const double* F, double* U, int* iteration
 int tp3d_solver_solve_begin(tp3d_solver* s, const double* F, double* U);
 int tp3d_solver_solve_end(tp3d_solver* s, int* iterations, double* relres, int* replaced);
 
+/* Initial guess of the next solve from the last two solutions of the same load
+ * case, for the operator of the current density (call after set_density): U <-
+ * a U + b U_prev with (a, b) minimising the energy x'Kx / 2 - F'x over span{U,
+ * U_prev} (a 2x2 Galerkin system on the device: two FP64 operator applies and
+ * one fused reduction), U_prev <- the old U.  With have_prev = 0 only U_prev is
+ * updated.  The span holds the linear extrapolation 2 U - U_prev of
+ * tp3d_warm_start, so the start is at least as close in the energy norm; on the
+ * 128x64x64 workload it saves 1-3 CG iterations per solve.  Replaces the
+ * reference's cold spsolve (pytopo3d/core/optimizer.py:592), which has no
+ * initial guess.  Needs a solver created with ritz_start = 1. */
+int tp3d_solver_ritz_start(tp3d_solver* s, const double* F, double* U, double* U_prev, int have_prev);
 int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
 int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
 /* Coarse level `level` (1 .. levels - 2) of the mixed form's multigrid applied as

@@ -63,6 +63,7 @@ class SolverOpts(C.Structure):
         ("cluster_cycle", i32),
         ("fine_slab_depth", i32),
         ("coarse_node_major", i32),
+        ("ritz_start", i32),
     ]
 
 
@@ -119,6 +120,7 @@ SIGNATURES = {
     "tp3d_solver_apply_f64": (i32, [vp, vp, vp]),
     "tp3d_solver_apply_f32": (i32, [vp, vp, vp]),
     "tp3d_solver_apply_level_f32": (i32, [vp, i32, vp, vp]),
+    "tp3d_solver_ritz_start": (i32, [vp, vp, vp, vp, i32]),
     "tp3d_solver_time_apply": (i32, [vp, i32, i32, C.POINTER(f64)]),
     "tp3d_solver_autotune": (i32, [vp, vp, vp, i32, C.POINTER(f64), i32]),
     "tp3d_solver_time_level": (i32, [vp, i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),

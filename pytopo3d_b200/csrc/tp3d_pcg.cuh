@@ -266,6 +266,86 @@ __global__ void warm_start_dev_kernel(long long n, double* U, double* U_prev, co
   }
 }
 
+// Rayleigh-Ritz initial guess from the last two solutions U1 = U and
+// U2 = U_prev under the current operator K: the x = a U1 + b U2 that minimises
+// the energy x'Kx / 2 - F'x over span{U1, U2}, which contains the linear
+// extrapolation 2 U1 - U2 of warm_start_kernel, so it starts CG at least as
+// close in the energy norm.  Gate: whether both solutions exist (the host's
+// flag, or the stage counters' history test when ctr is given).
+__global__ void ritz_gate_kernel(int* gate, int have_prev, const int* ctr) {
+  *gate = ctr ? (ctr[kStBase] + ctr[kStIter] >= 2) : (have_prev != 0);
+}
+
+// Per-block sums of U1.KU1, U1.KU2, U2.KU2, F.U1, F.U2 (q1 = K U1, q2 = K U2;
+// fixed DOFs of U are zero, so they add nothing); the last block adds the
+// partials in a fixed order and solves the 2x2 Galerkin system for (a, b).  A
+// nearly dependent pair (det <= 1e-10 G11 G22) falls back to the best multiple
+// of U1, anything non-finite to U1 itself.
+__global__ void ritz_dot_kernel(long long n, const double* __restrict__ F, const double* __restrict__ U1,
+                                const double* __restrict__ U2, const double* __restrict__ q1,
+                                const double* __restrict__ q2, const int* gate, double* partials,
+                                unsigned int* count, double* coef) {
+  if (*(volatile const int*)gate == 0) return;
+  __shared__ double red[32];
+  __shared__ int s_last;
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double a = U1[i], b = U2[i], f = F[i], x = q1[i], y = q2[i];
+    v[0] = fma(a, x, v[0]);
+    v[1] = fma(a, y, v[1]);
+    v[2] = fma(b, y, v[2]);
+    v[3] = fma(f, a, v[3]);
+    v[4] = fma(f, b, v[4]);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double t = block_sum(v[k], red);
+    if (threadIdx.x == 0) partials[k * gridDim.x + blockIdx.x] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(count, 1u) == gridDim.x - 1u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double tot[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    double t = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += __ldcg(&partials[k * gridDim.x + i]);
+    tot[k] = block_sum(t, red);
+  }
+  if (threadIdx.x == 0) {
+    const double g11 = tot[0], g12 = tot[1], g22 = tot[2], r1 = tot[3], r2 = tot[4];
+    double a = 1.0, b = 0.0;
+    const double det = g11 * g22 - g12 * g12;
+    if (g11 > 0.0 && g22 > 0.0 && det > 1e-10 * g11 * g22) {
+      a = (r1 * g22 - r2 * g12) / det;
+      b = (g11 * r2 - g12 * r1) / det;
+    } else if (g11 > 0.0) {
+      a = r1 / g11;
+    }
+    if (!isfinite(a) || !isfinite(b)) {
+      a = 1.0;
+      b = 0.0;
+    }
+    coef[0] = a;
+    coef[1] = b;
+    *count = 0u;
+  }
+}
+
+// U <- a U1 + b U2 where the gate is open (else U stays U1), U_prev <- U1.
+__global__ void ritz_combine_kernel(long long n, double* U, double* U_prev, const double* coef, const int* gate) {
+  const bool on = *(volatile const int*)gate != 0;
+  const double a = on ? coef[0] : 1.0, b = on ? coef[1] : 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double u1 = U[i], u2 = U_prev[i];
+    if (on) U[i] = a * u1 + b * u2;
+    U_prev[i] = u1;
+  }
+}
+
 // After a queued mixed solve: whether the host path would have accepted it
 // without its FP64 fallback (converged, or at its residual floor).  Otherwise
 // *abort is raised.  The solve's CG iterations are summed into *cg.

@@ -338,6 +338,10 @@ struct tp3d_solver {
   int clu_L = 0, clu_C = 0;
   size_t clu_smem = 0;
   __nv_bfloat16* clu_SN = nullptr;  // level clu_L's node-major bf16 stencil
+  // Rayleigh-Ritz initial guess (o.ritz_start): K U1, K U2, gate, partials, arrivals, (a, b)
+  double *rz_q1 = nullptr, *rz_q2 = nullptr, *rz_part = nullptr, *rz_coef = nullptr;
+  int* rz_gate = nullptr;
+  unsigned int* rz_count = nullptr;
   int cyc_blocks64 = 0, cyc_blocks32 = 0;
   unsigned int* cyc_bar = nullptr;  // [barrier word, error]
   std::vector<void*> allocs;
@@ -403,6 +407,32 @@ struct tp3d_solver {
     if constexpr (sizeof(T) == 8) return 8.0;
     else return rho16 ? 2.0 : 4.0;
   }
+  // Rayleigh-Ritz initial guess for the next solve (ritz_gate_kernel and the
+  // kernels after it): U <- a U + b U_prev minimising the energy under the
+  // current operator, U_prev <- the old U.  Queued on the solver's stream, the
+  // gate read on the device, so a stage graph captures the same kernels.
+  int ritz_start(const double* F, double* U, double* U_prev, int have_prev, const int* ctr) {
+    if (!rz_q1) return TP3D_ERR_ARG;
+    const long long ndof = 3 * g.nnode();
+    const int nb = grid_blocks(ndof);
+    ritz_gate_kernel<<<1, 1, 0, st>>>(rz_gate, have_prev, ctr);
+    count_launch();
+    OpIO<double> io;
+    io.u = U;
+    io.out = rz_q1;
+    io.gate = rz_gate;
+    if (int rc = fine<double, kModeApply>(io)) return rc;
+    io.u = U_prev;
+    io.out = rz_q2;
+    if (int rc = fine<double, kModeApply>(io)) return rc;
+    ritz_dot_kernel<<<nb, 256, 0, st>>>(ndof, F, U, U_prev, rz_q1, rz_q2, rz_gate, rz_part, rz_count, rz_coef);
+    ritz_combine_kernel<<<nb, 256, 0, st>>>(ndof, U, U_prev, rz_coef, rz_gate);
+    count_launch();
+    count_launch();
+    TP3D_CHECK_LAUNCH();
+    return TP3D_OK;
+  }
+
   template <typename T, int MODE>
   int fine(const OpIO<T>& io) {
     count_bytes(op_bytes<T, MODE>(3 * g.nnode(), g.nnode(), fine_src_bytes<T>() * (double)g.nele()));
@@ -1861,6 +1891,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->cluster_cycle = 1;
   o->fine_slab_depth = 0;
   o->coarse_node_major = 1;
+  o->ritz_start = 1;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1956,6 +1987,16 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   s->partials = s->alloc<double>(kMaxPartials);
   s->fin_count = s->alloc<unsigned int>(1);
   if (s->fin_count) cudaMemset(s->fin_count, 0, sizeof(unsigned int));
+  if (o.ritz_start) {
+    const long long ndof = 3 * s->g.nnode();
+    s->rz_q1 = s->alloc<double>(ndof);
+    s->rz_q2 = s->alloc<double>(ndof);
+    s->rz_part = s->alloc<double>(5 * (size_t)s->grid_blocks(ndof));
+    s->rz_coef = s->alloc<double>(2);
+    s->rz_gate = s->alloc<int>(1);
+    s->rz_count = s->alloc<unsigned int>(1);
+    if (s->rz_count) cudaMemset(s->rz_count, 0, sizeof(unsigned int));
+  }
   s->loop_passes = s->alloc<unsigned int>(1);
   // The side stream (element chain, coarsest stencil and inverse: the longest
   // chain of the set-up) gets the highest priority, so that its blocks are
@@ -2655,6 +2696,17 @@ extern "C" int tp3d_solver_autotune(tp3d_solver* s, const double* F, const doubl
   return TP3D_OK;
 }
 
+extern "C" int tp3d_solver_ritz_start(tp3d_solver* s, const double* F, double* U, double* U_prev, int have_prev) {
+  if (!s || !F || !U || !U_prev || !s->have_density) return TP3D_ERR_ARG;
+  if (!s->rz_q1) {
+    tp3d_set_last_error("the solver was created without ritz_start");
+    return TP3D_ERR_ARG;
+  }
+  if (int rc = s->enter()) return rc;
+  if (int rc = s->ritz_start(F, U, U_prev, have_prev, nullptr)) return rc;
+  return s->leave();
+}
+
 extern "C" int tp3d_warm_start(double* U, double* U_prev, long long n, int have_prev, void* stream) {
   if (!U || !U_prev || n < 0) return TP3D_ERR_ARG;
   if (n == 0) return TP3D_OK;
@@ -2754,13 +2806,28 @@ int stage_body(tp3d_solver* s, const tp3d_stage_desc* d, cudaStream_t cs, cudaSt
   const long long ndof = 3 * g.nnode(), nele = g.nele();
   const int nb = s->grid_blocks(ndof);
   int* ctr = d->counters;
-  for (int k = 0; k < d->ncases; ++k) {
-    double* U = d->U + (size_t)k * ndof;
-    warm_start_dev_kernel<<<nb, 256, 0, cs>>>(ndof, U, d->U_prev + (size_t)k * ndof, ctr);
-    TP3D_CHECK(cudaMemcpyAsync(d->U_bak + (size_t)k * ndof, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+  if (s->rz_q1) {
+    // Rayleigh-Ritz start: it needs the new operator, so the set-up comes first
+    // (the host path's order); the history test is read from the counters
+    if (int rc = tp3d_solver_set_density(s, d->rho_p, d->penal)) return rc;
+    for (int k = 0; k < d->ncases; ++k) {
+      double* U = d->U + (size_t)k * ndof;
+      if (int rc = s->enter()) return rc;
+      if (int rc = s->ritz_start(d->F + (size_t)k * ndof, U, d->U_prev + (size_t)k * ndof, 0, ctr)) return rc;
+      if (int rc = s->leave()) return rc;
+      TP3D_CHECK(cudaMemcpyAsync(d->U_bak + (size_t)k * ndof, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 cs));
+    }
+  } else {
+    for (int k = 0; k < d->ncases; ++k) {
+      double* U = d->U + (size_t)k * ndof;
+      warm_start_dev_kernel<<<nb, 256, 0, cs>>>(ndof, U, d->U_prev + (size_t)k * ndof, ctr);
+      TP3D_CHECK(cudaMemcpyAsync(d->U_bak + (size_t)k * ndof, U, ndof * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 cs));
+    }
+    *body_kernels += d->ncases;
+    if (int rc = tp3d_solver_set_density(s, d->rho_p, d->penal)) return rc;
   }
-  *body_kernels += d->ncases;
-  if (int rc = tp3d_solver_set_density(s, d->rho_p, d->penal)) return rc;
   for (int k = 0; k < d->ncases; ++k)
     if (int rc = s->solve_into_capture(d->F + (size_t)k * ndof, d->U + (size_t)k * ndof, ctr + kStAbort,
                                        ctr + kStCg))

@@ -169,8 +169,14 @@ class SimpState:
         iters = 0
         for k in range(self.F.shape[0]):
             if not rerun:
-                _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
-                                             1 if self.n_solved >= 2 else 0, _lib.stream_ptr()), "warm_start")
+                have_prev = 1 if self.n_solved >= 2 else 0
+                if self.solver.opts.ritz_start:
+                    # the best combination of the last two solutions under the new operator
+                    _lib.check(L.tp3d_solver_ritz_start(self.solver._h, self.F[k].data_ptr(), self.U[k].data_ptr(),
+                                                        self.U_prev[k].data_ptr(), have_prev), "ritz_start")
+                else:
+                    _lib.check(L.tp3d_warm_start(self.U[k].data_ptr(), self.U_prev[k].data_ptr(), self.U.shape[1],
+                                                 have_prev, _lib.stream_ptr()), "warm_start")
             dst_dc = self.dc_dx if k == 0 else self.dc_acc
             if k == 0 and self.solver.autotune_pending and self.n_iter + 1 >= self.solver.autotune_at:
                 self.solver.autotune(self.F[k], self.U[k])

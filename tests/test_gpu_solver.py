@@ -651,3 +651,51 @@ def test_autotune_picks_measured_degrees_and_caches_them(P, precision, criterion
     assert s2.stats()["autotuned"] == 2
     for h in (ref, s, s2):
         h.close()
+
+
+# Rayleigh-Ritz start (tp3d_solver_ritz_start): for the new operator, the
+# combination of the last two solutions has an energy x'Kx/2 - F'x no higher
+# than the linear extrapolation 2 U1 - U2 or U1 (both lie in the same span), the
+# history is rotated (U_prev <- U1), and without history U is left as it is.
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_ritz_start_lowers_the_energy_of_the_initial_guess(P, prec):
+    from pytopo3d_b200 import _lib
+    from pytopo3d_b200._tensors import to_flat
+    from pytopo3d_b200.solver import HexSolver
+
+    nx, ny, nz = 24, 12, 12
+    KE = P.lk_H8(elem_size=1.0)
+    rho, free, fmask = _problem(nx, ny, nz, seed=21, lo=0.05)
+    F = torch.as_tensor(O.build_force_vector(nx, ny, nz, fmask.size)).cuda()
+    s = HexSolver(nx, ny, nz, KE, fmask, precision=prec)
+    assert s.opts.ritz_start == 1
+    sols = []
+    for scale in (1.0, 0.97, 0.94):
+        r = np.clip(rho * scale, 0.01, 1.0)
+        s.set_density(to_flat(r), 3.0)
+        sols.append(s.solve(F).clone())
+    U1, U2 = sols[1], sols[0]
+    # the third density's operator is current (its solve is in sols[2])
+
+    def energy(x):
+        y = s.apply(x)
+        return 0.5 * float(x @ y) - float(F @ x)
+
+    L = _lib.lib()
+    U, Up = U1.clone(), U2.clone()
+    _lib.check(L.tp3d_solver_ritz_start(s._h, F.data_ptr(), U.data_ptr(), Up.data_ptr(), 1), "ritz_start")
+    torch.cuda.synchronize()
+    assert torch.equal(Up, U1)
+    e_ritz, e_ext, e_last = energy(U), energy(2 * U1 - U2), energy(U1)
+    assert e_ritz <= e_ext + 1e-12 * abs(e_ext) and e_ritz <= e_last + 1e-12 * abs(e_last)
+    # no history: U unchanged, U_prev takes it
+    U, Up = U1.clone(), torch.zeros_like(U1)
+    _lib.check(L.tp3d_solver_ritz_start(s._h, F.data_ptr(), U.data_ptr(), Up.data_ptr(), 0), "ritz_start")
+    torch.cuda.synchronize()
+    assert torch.equal(U, U1) and torch.equal(Up, U1)
+    s.close()
+    # without the option the entry point is refused and the loops use the extrapolation
+    s0 = HexSolver(nx, ny, nz, KE, fmask, precision=prec, ritz_start=0)
+    s0.set_density(to_flat(rho), 3.0)
+    assert L.tp3d_solver_ritz_start(s0._h, F.data_ptr(), U.data_ptr(), Up.data_ptr(), 1) == _lib.TP3D_ERR_ARG
+    s0.close()
