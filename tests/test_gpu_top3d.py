@@ -277,3 +277,31 @@ def test_cantilever_full_run_matches_reference(cantilever_run):
                                atol=1e-12)
     np.testing.assert_allclose([s["final_change"] for s in st], g["cl_stage_final_change"], atol=5e-7)
     assert diag["binary_compliance"] == pytest.approx(float(g["cl_binary_compliance"]), rel=1e-6)
+
+
+def test_step_host_matches_device_loop(P):
+    """SimpLoop.step_host (host design in, host design and compliance out, the
+    path bench.py's end-to-end figure times) gives the device loop's trajectory
+    bit for bit, for flat and (nely, nelx, nelz) host designs."""
+    import bench
+    from pytopo3d_b200.optimizer import SimpLoop
+
+    nelx, nely, nelz = 24, 12, 12
+    shape, solid, void, F, fixed = bench.workload(nelx, nely, nelz)
+    loops = [SimpLoop(nelx, nely, nelz, 0.3, 3.0, 2.0, P.lk_H8(elem_size=1.0), F, fixed, solid, void,
+                      precision="fp64") for _ in range(2)]
+    for lp in loops:
+        lp.set_beta(1.0)
+    x_host = loops[1].design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
+    for it in range(4):
+        st = loops[0].step()
+        if it % 2 == 0:
+            x_host, c = loops[1].step_host(x_host)
+        else:  # the 3D layout of the reference's arrays
+            x3 = x_host.reshape(nelz, nelx, nely).transpose(2, 1, 0)
+            x_host, c = loops[1].step_host(x3)
+        assert c == float(st[0])
+        ref = loops[0].design().permute(2, 1, 0).contiguous().reshape(-1).cpu().numpy()
+        assert np.array_equal(x_host, ref)
+    for lp in loops:
+        lp.close()
