@@ -315,7 +315,10 @@ int tp3d_solver_solve_end(tp3d_solver* s, int* iterations, double* relres, int* 
  * tp3d_warm_start, so the start is at least as close in the energy norm; on the
  * 128x64x64 workload it saves 1-3 CG iterations per solve.  Replaces the
  * reference's cold spsolve (pytopo3d/core/optimizer.py:592), which has no
- * initial guess.  Needs a solver created with ritz_start = 1. */
+ * initial guess.  F, U, U_prev: device FP64 vectors of the grid's 3 x nodes
+ * DOFs (fixed DOFs of U and U_prev zero, as the solves leave them); queued on
+ * the solver's stream after the caller's stream.  Needs a solver created with
+ * ritz_start = 1. */
 int tp3d_solver_ritz_start(tp3d_solver* s, const double* F, double* U, double* U_prev, int have_prev);
 int tp3d_solver_apply_f64(tp3d_solver* s, const double* u, double* y);
 int tp3d_solver_apply_f32(tp3d_solver* s, const float* u, float* y);
