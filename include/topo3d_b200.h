@@ -193,12 +193,13 @@ typedef struct tp3d_solver_opts {
   int coarsest_max_dofs;/* stop coarsening at or below this many DOFs */
   int max_levels;       /* cap on multigrid levels (1 = Jacobi-PCG only) */
   int smoother;         /* 0 Chebyshev(Jacobi) with power-iteration bounds, 1 damped Jacobi */
-  double cheb_ratio;    /* Chebyshev interval [lambda_max / ratio, lambda_max] */
+  double cheb_ratio;    /* Chebyshev interval [lambda_max / ratio, lambda_max] (default 30) */
   int power_iterations; /* power iterations per level for lambda_max(Dinv A) */
   int inner_density;    /* mixed: FP32 fine operator from 0 = FP32 moduli, 1 = BF16 densities */
   double reliable_delta;/* mixed: replace the FP32 residual by the FP64 one when it fell by this factor
-                           (default 0.01: on the 128x64x64 step two replacements per solve instead of
-                           four at 0.05, same CG iterations and final FP64 residual, 1.5% faster) */
+                           (default 0.05; 0.01 measured 1.5% faster on the 128x64x64 step, but the
+                           FP32 residual then drifts further from the FP64 one between
+                           replacements, and a solve ended 2% above rtol) */
   int max_restarts;     /* FP64: restarts from the true residual when the recursive one drifted */
   int fine_operator;    /* fine-level K u: 0 the fastest of the dense-KE form and the Walsh-Hadamard
                            block form's launch shapes, tile shapes (the three with the fewest blocks

@@ -1873,7 +1873,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->cheb_ratio = 30.0;
   o->power_iterations = 12;
   o->inner_density = 0;
-  o->reliable_delta = 0.01;
+  o->reliable_delta = 0.05;
   o->max_restarts = 3;
   o->fine_operator = 0;
   o->fused_cycle_dofs = 0;
