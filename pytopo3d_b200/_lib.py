@@ -64,6 +64,7 @@ class SolverOpts(C.Structure):
         ("fine_slab_depth", i32),
         ("coarse_node_major", i32),
         ("ritz_start", i32),
+        ("cheb_ratio_coarse", C.c_double),
     ]
 
 

@@ -1892,6 +1892,7 @@ extern "C" void tp3d_solver_default_opts(tp3d_solver_opts* o) {
   o->fine_slab_depth = 0;
   o->coarse_node_major = 1;
   o->ritz_start = 1;
+  o->cheb_ratio_coarse = 0.0;
 }
 
 extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE_host, const uint8_t* fixed_dofs,
@@ -1910,7 +1911,8 @@ extern "C" int tp3d_solver_create(int nelx, int nely, int nelz, const double* KE
   tp3d_solver_opts& o = s->o;
   if (o.pre_sweeps < 1 || o.pre_sweeps > kMaxCheb || o.post_sweeps < 0 || o.post_sweeps > kMaxCheb ||
       o.max_iterations < 1 || !(o.rtol > 0.0) || o.coarsest_max_dofs < 1 || o.max_levels < 1 ||
-      !(o.cheb_ratio > 1.0) || o.power_iterations < 2 || !(o.reliable_delta > 0.0 && o.reliable_delta < 1.0))
+      !(o.cheb_ratio > 1.0) || !(o.cheb_ratio_coarse == 0.0 || o.cheb_ratio_coarse > 1.0) ||
+      o.power_iterations < 2 || !(o.reliable_delta > 0.0 && o.reliable_delta < 1.0))
     return fail(TP3D_ERR_ARG, "invalid solver options");
   if (o.coarse_sweeps < 0 || o.coarse_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid coarse_sweeps");
   if (o.deep_sweeps < 0 || o.deep_sweeps > kMaxCheb) return fail(TP3D_ERR_ARG, "invalid deep_sweeps");
@@ -2236,7 +2238,8 @@ static int spectra_level(tp3d_solver* s, int L, cudaStream_t ps) {
   if (rc == TP3D_OK) {
     dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], w[cur], pa, nullptr, nullptr);
     dot_kernel<T><<<nb, 256, 0, st>>>(ndof, w[1 - cur], w[1 - cur], pb, nullptr, nullptr);
-    cheb_setup_kernel<<<1, 256, 0, st>>>(pa, nb, pb, nb, s->o.cheb_ratio, 1.1, s->coef[L]);
+    const double ratio = (L >= 1 && s->o.cheb_ratio_coarse > 0.0) ? s->o.cheb_ratio_coarse : s->o.cheb_ratio;
+    cheb_setup_kernel<<<1, 256, 0, st>>>(pa, nb, pb, nb, ratio, 1.1, s->coef[L]);
     scale_copy_kernel<T><<<nb, 256, 0, st>>>(ndof, w[cur], s->coef[L] + kCoefLen - 1, s->pv[L]);
     for (int i = 0; i < 4; ++i) count_launch();
     rc = cuda_status(cudaGetLastError());
